@@ -1,0 +1,388 @@
+"""Benchmark of the LJ timestep hot path (one JSON line on rank 0).
+
+Workload: 2,048,000 atoms, FCC 80^3 cells at rho = 0.8442 (L = 134.37),
+T = 0.722 Maxwell-Boltzmann from a seed, smoothed LJ with rc = 2.5, search
+length 2.8, dt = 0.004, NVE.  One bench step is one observation interval of
+the reference's Benchmark project (ObserveLoop = 100 MD steps of
+MDManager::Calculate, src/benchmark.cc:32-41), rebuilds included as they
+fall due.  The headline path is FP32-mixed (FP32 pair forces, FP64
+integration and reductions); the plain FP64 drop-in is measured beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mdg|reference]
+
+Under torchrun (N > 1) every rank runs its own replica (weak scaling, no
+data-path collective); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import pathlib
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "LJ atom-steps/s at 2.05M atoms, FP32-mixed vs FP64 on 1 B200; force err"
+UNIT = "atom-steps/s"
+MD_STEPS_PER_STEP = 100
+L2_BYTES = 126 * 2 ** 20
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------ distributed
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws, backend):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def max_over_ranks(dist, value, device=None):
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device=None):
+    if dist is not None:
+        if device is not None and str(device).startswith("cuda"):
+            dist.barrier(device_ids=[int(str(device).split(":")[1])])
+        else:
+            dist.barrier()
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in pathlib.Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# -------------------------------------------------------------- reference
+def ref_threads():
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    return max(1, min(cores, 256))
+
+
+def local_grid(t, L, sl):
+    """Factor t threads into an lx*ly*lz unit grid with every unit at least
+    2*SearchLength wide (ParaInfo only factors powers of two by itself,
+    src/parainfo.cc:44-58)."""
+    best = None
+    for lx in range(1, t + 1):
+        if t % lx:
+            continue
+        for ly in range(1, t // lx + 1):
+            if (t // lx) % ly:
+                continue
+            lz = t // lx // ly
+            if min(L[0] / lx, L[1] / ly, L[2] / lz) < 2 * sl:
+                continue
+            score = max(lx, ly, lz)
+            if best is None or score < best[0]:
+                best = (score, (lx, ly, lz))
+    return best[1] if best else None
+
+
+def run_reference_bench(state, steps, warmup, threads):
+    """Times the reference's own CPU build (AVX2, oracle/_ref) on the state
+    through its OracleBench project; returns (atom_steps_per_s, info)."""
+    from oracle import lj_oracle as O
+
+    t = threads
+    grid = local_grid(t, state.L, state.rc + 0.3)
+    while grid is None or t < 3:  # the reference caps each unit at 1e6 atoms incl. ghosts
+        t -= 1 if t > 3 else -1
+        grid = local_grid(t, state.L, state.rc + 0.3)
+    extra = {"Steps": str(steps), "Warmup": str(warmup), "LocalGridX": str(grid[0]),
+             "LocalGridY": str(grid[1]), "LocalGridZ": str(grid[2])}
+    wd, out = O.run_reference("OracleBench", state.q, state.v, state.ids, state.L, state.rc, state.dt,
+                              flavour="avx2", threads=t, extra=extra, timeout=1800)
+    line = [x for x in out.splitlines() if x.startswith("ORACLE_BENCH")][-1].split()
+    kv = {line[i]: float(line[i + 1]) for i in range(1, len(line) - 1, 2)}
+    # ConstructionCounter sums over the units, which all rebuild together
+    return kv["atom_steps_per_s"], {"cores": t, "grid": grid, "sec": kv["sec"], "steps": int(kv["steps"]),
+                                    "rebuilds": int(round(kv["rebuilds"] / kv["units"]))}
+
+
+def ref_sample_steps(cores, seconds):
+    # about 2.6e6 atom-steps/s per core for the AVX2 build at this density
+    est = 2.6e6 * cores
+    return int(min(2000, max(10, seconds * est / 2.048e6)))
+
+
+# -------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["mdg", "reference"], default="mdg")
+    ap.add_argument("--md-steps-per-step", type=int, default=MD_STEPS_PER_STEP)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cells", type=int, default=80, help="FCC cells per axis (80 = 2,048,000 atoms)")
+    args = ap.parse_args()
+    ws, rank, local = dist_env()
+    from mdacp_b200 import workloads as W
+
+    state = W.fcc_liquid(args.cells, 0.8442, 0.722, seed=2026 + rank, rc=2.5, dt=0.004,
+                         name=f"lj_fcc{4 * args.cells ** 3}_rho0.8442")
+    n = state.n
+    config = {
+        "workload": f"{state.name}: {n} atoms, FCC {args.cells}^3 cells, rho 0.8442, L {state.L[0]:.4f}, "
+                    "T 0.722, rc 2.5, search length 2.8, dt 0.004, NVE",
+        "n_atoms": n, "rho": 0.8442, "temperature": 0.722, "rc": 2.5, "search_length": 2.8, "dt": 0.004,
+        "md_steps_per_step": args.md_steps_per_step,
+        "l2": "inputs larger than L2 (state 131 MB + pairlist > 1 GB per replica)",
+        "parallelism": "replicas" if args.gpus > 1 else "single",
+    }
+    if args.impl == "reference":
+        return main_reference(args, ws, rank, state, config)
+    return main_mdg(args, ws, rank, local, state, config)
+
+
+def main_reference(args, ws, rank, state, config):
+    if rank != 0:
+        return 0
+    cores = ref_threads()
+    md_steps = ref_sample_steps(cores, 60.0)
+    value, info = run_reference_bench(state, md_steps, max(1, min(args.warmup, 5)), cores)
+    ms_per_md = 1e3 * state.n / value
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": info["steps"],
+        "warmup": max(1, min(args.warmup, 5)), "ms_per_step": ms_per_md, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": dict(config, md_steps_per_step=1, precision="fp64 (reference AVX2 CPU build)",
+                       unit_grid=list(info["grid"])),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": "reference",
+                         "sample": f"{info['steps']} MD steps of the full {state.n}-atom system "
+                                   f"({info['rebuilds']} rebuilds, {info['sec']:.2f} s), OpenMP units "
+                                   f"{info['grid']}, 1 MPI rank"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def force_kernel_bytes(n, list_entries, precision):
+    """Algorithmic bytes of one force-kick launch (neighbour gathers count as
+    cache-served): own position + row length + list + velocity read/write."""
+    own = 16 if precision == "fp32" else 32
+    return n * (own + 4 + 32 + 32) + 4 * list_entries
+
+
+def timed_run(sys_, args, dist, device, torch):
+    """W warm-up + K timed bench steps of md_steps_per_step MD steps."""
+    mdn = args.md_steps_per_step
+    for _ in range(args.warmup):
+        sys_.calculate(mdn)
+    sys_.set_kernel_timing(True)
+    info0 = sys_.info()
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(sys_.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sys_.calculate(mdn)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(dist, device)
+    ms = e0.elapsed_time(e1)
+    info1 = sys_.info()
+    fms, flaunch, klaunch = sys_.kernel_time()
+    sys_.set_kernel_timing(False)
+    launches = klaunch + 8 * (info1["rebuilds"] - info0["rebuilds"]) + 3 * (
+        info1["displacement_checks"] - info0["displacement_checks"])
+    return ms, fms, flaunch, launches, info0, info1
+
+
+def main_mdg(args, ws, rank, local, state, config):
+    import torch
+
+    import mdacp_b200 as M
+
+    dist = init_dist(ws, "nccl")
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    n = state.n
+    sampler = ClockSampler(local)
+    result = {}
+    for prec_name, prec in (("fp32", M.FP32_MIXED), ("fp64", M.FP64)):
+        s = M.System(state.L, cutoff=state.rc, time_step=state.dt, capacity=n, precision=prec, device=local)
+        s.set_state(state.q, state.v)
+        if prec_name == "fp32":
+            sampler.start()
+        ms, fms, flaunch, launches, info0, info1 = timed_run(s, args, dist, device, torch)
+        if prec_name == "fp32":
+            clocks = sampler.stop()
+        ms_max = max_over_ranks(dist, ms, device)
+        md_steps = args.steps * args.md_steps_per_step
+        result[prec_name] = dict(ms=ms_max, value=ws * n * md_steps / (ms_max * 1e-3), force_ms=fms,
+                                 force_launches=flaunch, launches=launches, info0=info0, info1=info1)
+        s.close()
+
+    # end to end through the C ABI from pinned host buffers (FP32-mixed path)
+    s = M.System(state.L, cutoff=state.rc, time_step=state.dt, capacity=n, precision=M.FP32_MIXED, device=local)
+    hq = torch.empty((n, 4), dtype=torch.float64, pin_memory=True).numpy()
+    hv = torch.empty((n, 4), dtype=torch.float64, pin_memory=True).numpy()
+    hq[:, :3] = state.q
+    hq[:, 3] = 0.0
+    hv[:, :3] = state.v
+    hv[:, 3] = 0.0
+    for _ in range(max(1, min(args.warmup, 2))):
+        s.set_state4(hq, hv)
+        s.calculate(args.md_steps_per_step)
+        s.get_state4(hq, hv)
+    barrier(dist, device)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.set_state4(hq, hv)
+        s.calculate(args.md_steps_per_step)
+        s.get_state4(hq, hv)
+    t_e2e = time.perf_counter() - t0
+    t_e2e = max_over_ranks(dist, t_e2e, device)
+    s.close()
+    e2e_value = ws * n * args.steps * args.md_steps_per_step / t_e2e
+
+    # FP32-mixed force error against FP64 at full size
+    errs = {}
+    sa = M.System(state.L, cutoff=state.rc, time_step=state.dt, capacity=n, precision=M.FP64, device=local)
+    sa.set_state(state.q, state.v)
+    sa.calculate(50)
+    q, v = sa.state_by_id()
+    f64 = sa.forces_by_id()
+    sa.close()
+    sb = M.System(state.L, cutoff=state.rc, time_step=state.dt, capacity=n, precision=M.FP32_MIXED, device=local)
+    sb.set_state(q, v)
+    f32 = sb.forces_by_id()
+    sb.close()
+    d = np.linalg.norm(f32 - f64, axis=1)
+    mag = np.linalg.norm(f64, axis=1)
+    errs = {"max": float(d.max() / max(mag.max(), np.sqrt((mag ** 2).mean()))),
+            "rms": float(np.sqrt((d ** 2).mean()) / np.sqrt((mag ** 2).mean())),
+            "state": "after 50 FP64 steps from the start state"}
+
+    r32, r64 = result["fp32"], result["fp64"]
+    hbm, peak_kind = peaks()
+    rebuilds = r32["info1"]["rebuilds"] - r32["info0"]["rebuilds"]
+    entries = r32["info1"]["list_entries"]
+    fbytes = force_kernel_bytes(n, entries, "fp32")
+    f_avg_ms = r32["force_ms"] / max(1, r32["force_launches"])
+    achieved = fbytes / (f_avg_ms * 1e-3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "force_fp32_c2.json"
+    if prof.exists():
+        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+    line = {
+        "metric": METRIC, "value": r32["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r32["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": dict(config, precision="fp32_mixed: FP32 pair forces on fixed-point minimum-image "
+                                         "displacements, FP64 per-atom sums, integration and reductions",
+                       rebuilds=rebuilds, mean_row=entries / n),
+        "fp64": {"value": r64["value"], "ms_per_md_step": r64["ms"] / (args.steps * args.md_steps_per_step),
+                 "speedup_fp32_over_fp64": r32["value"] / r64["value"]},
+        "ms_per_md_step": r32["ms"] / (args.steps * args.md_steps_per_step),
+        "force_error_fp32_vs_fp64": errs,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic, "kernel": "k_force_fp32 (kick)",
+                     "algorithmic_bytes_per_launch": fbytes, "avg_launch_ms": f_avg_ms,
+                     "launches": r32["force_launches"], "peak_kind": peak_kind},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 32 * n,
+                "d2h_bytes_per_step": 2 * 32 * n},
+        "gpu_launches": r32["launches"],
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline and ws == 1:
+        try:
+            cores = ref_threads()
+            v, info = run_reference_bench(state, ref_sample_steps(cores, 15.0), 2, cores)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "reference",
+                                    "sample": f"{info['steps']} MD steps of the same {n}-atom system, "
+                                              f"reference AVX2 build, {info['sec']:.2f} s"}
+        except Exception as exc:  # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
+                                    "sample": f"not run: {exc}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,175 @@
+/*
+ * mdacp_b200 -- C ABI of the B200-native Lennard-Jones timestep.
+ *
+ * One handle owns one periodic single-domain system resident in the GPU's
+ * HBM: cell-sorted positions and velocities, the Verlet pairlist, the skin
+ * bookkeeping and the step graph.  Plain pointers and sizes only; host
+ * arrays use the reference's padded AoS layout (x, y, z, pad per atom, as
+ * double q[N][D] / p[N][D] with D = 4, include/mdconfig.h:9, include/variables.h:19-28).
+ *
+ * Each entry point names the reference interface it replaces
+ * (kohnakagawa/mdacp, path:line).  Every call returns an mdg_status; 0 is
+ * success, negative values are errors whose text mdg_last_error() returns.
+ * The reference reports the same conditions with show_error + exit(1)
+ * (include/mdconfig.h:37); the drop-in C++ classes map a negative status
+ * back onto that behaviour.
+ *
+ * A handle is not thread-safe.  Separate handles are independent.  All work
+ * is issued on the handle's stream; calls that return host data synchronise
+ * that stream.
+ */
+#ifndef MDACP_B200_H
+#define MDACP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mdg_handle mdg_handle;
+typedef int mdg_status;
+
+enum {
+  MDG_OK = 0,
+  MDG_ERR_INVALID_ARGUMENT = -1,
+  MDG_ERR_CUDA = -2,
+  MDG_ERR_CAPACITY = -3,         /* atom or neighbour capacity exceeded */
+  MDG_ERR_TOO_FAST = -4,         /* 2 vmax dt > BufferLength (src/pairlist.cc:59-63) */
+  MDG_ERR_INVALID_POSITION = -5, /* atom outside [0,L] after wrap (src/variables.cc:75-83) */
+  MDG_ERR_NONFINITE = -6,        /* NaN / Inf in the state */
+  MDG_ERR_BOX_TOO_SMALL = -7,    /* fewer than 3 cells along an axis */
+  MDG_ERR_TIMEOUT = -8,          /* a bounded device wait gave up */
+  MDG_ERR_STATE = -9,            /* call out of order (e.g. no state uploaded) */
+  MDG_ERR_NO_DEVICE = -10
+};
+
+enum { MDG_FP64 = 0, MDG_FP32_MIXED = 1 };
+enum { MDG_NVE = 0, MDG_NOSE_HOOVER = 1, MDG_LANGEVIN = 2 };
+
+/* Run parameters; the reference's SimulationInfo public fields
+   (include/simulationinfo.h:20-33, src/simulationinfo.cc:5-51) plus the
+   compile-time CUTOFF_LENGTH (include/mdconfig.h:31), which is a runtime
+   value here. */
+typedef struct {
+  int capacity;             /* maximum number of atoms (reference: N, mdconfig.h:11) */
+  double L[3];              /* box lengths (SimulationInfo::L) */
+  double cutoff;            /* CUTOFF_LENGTH */
+  double buffer_length;     /* BufferLength (0.3); SearchLength = cutoff + buffer_length */
+  double time_step;         /* TimeStep */
+  int precision;            /* MDG_FP64 (drop-in) or MDG_FP32_MIXED */
+  int thermostat;           /* MDG_NVE, MDG_NOSE_HOOVER, MDG_LANGEVIN */
+  double aimed_temperature; /* AimedTemperature */
+  double heatbath_tau;      /* HeatbathTau */
+  double heatbath_gamma;    /* HeatbathGamma */
+  uint64_t seed;            /* Langevin noise key (Philox4x32-10) */
+  int check_list_length;    /* CheckListLength (500) */
+  int max_neighbors;        /* neighbour-row capacity; 0 = derived from density */
+  int device;               /* CUDA device ordinal */
+  void *stream;             /* cudaStream_t to issue work on; NULL = handle-owned stream */
+} mdg_params;
+
+/* Fills p with the reference defaults (SimulationInfo ctor, src/simulationinfo.cc:5-51). */
+void mdg_default_params(mdg_params *p);
+
+/* Replaces: MDUnit ctor allocation of Variables/MeshList/PairList and the
+   CUDA buffers (src/mdunit.cc:8-39, include/cuda_ptr.h:13-152,
+   src/meshlist.cu:21-33). */
+mdg_status mdg_create(const mdg_params *params, mdg_handle **out);
+mdg_status mdg_destroy(mdg_handle *h);
+
+/* Replaces: Variables::AddParticle for a whole array (src/variables.cc:35-47)
+   plus the per-step host-to-device copy (src/fcalculator.cu:5-13).  q4, v4 are
+   n x 4 doubles (pad ignored), type is n ints (may be NULL).  The list is
+   marked stale: the next step rebuilds it.  Atom slots are renumbered at every
+   rebuild (cell order); mdg_get_ids gives each slot's upload index. */
+mdg_status mdg_set_state(mdg_handle *h, const double *q4, const double *v4, const int *type,
+                         int n);
+/* Replaces: the device-to-host copy of p (src/fcalculator.cu:15-22) and reads
+   of Variables::q/p/type.  Arrays are in the current slot order. */
+mdg_status mdg_get_state(mdg_handle *h, double *q4, double *v4, int *type, int n);
+mdg_status mdg_get_ids(mdg_handle *h, int *ids, int n);
+mdg_status mdg_particle_number(mdg_handle *h, int *n);
+
+/* Replaces: MDManager::MakePairList (src/mdmanager.cc:387-417): wrap into
+   [0,L] (Variables::AdjustPeriodicBoundary, src/variables.cc:63-84), cell
+   counting sort (MeshList::MakeMesh, src/meshlist.cc:175-228), Verlet list
+   within SearchLength (MeshList::MakeList/SearchMesh, src/meshlist.cc:67-104,
+   242-292) and PairList::Init (src/pairlist.cc:10-23). */
+mdg_status mdg_make_pairlist(mdg_handle *h);
+
+/* Replaces: PairList::IsPairListExpired (src/pairlist.cc:25-45). */
+mdg_status mdg_check_expired(mdg_handle *h, int *expired);
+
+/* Replaces: ForceCalculator::UpdatePositionHalf (src/fcalculator.cc:17-30). */
+mdg_status mdg_update_position_half(mdg_handle *h);
+
+/* Replaces: ForceCalculator::CalculateForce (src/fcalculator.cc:32-50 and the
+   GPU offload src/fcalculator.cu:38-73): the kick p += F(q) * TimeStep. */
+mdg_status mdg_calculate_force(mdg_handle *h);
+
+/* Replaces: ForceCalculator::HeatbathZeta / HeatbathMomenta / Langevin
+   (src/fcalculator.cc:979-1017, src/fcalculator.cu:75-88). */
+mdg_status mdg_heatbath_zeta(mdg_handle *h, double current_temperature);
+mdg_status mdg_heatbath_momenta(mdg_handle *h);
+mdg_status mdg_langevin(mdg_handle *h);
+mdg_status mdg_get_zeta(mdg_handle *h, double *zeta);
+mdg_status mdg_set_zeta(mdg_handle *h, double zeta);
+
+/* Replaces: MDManager::Calculate (src/mdmanager.cc:153-186) called nsteps
+   times: expiry check, conditional rebuild, half drift, force kick (NVE,
+   Nose-Hoover or Langevin branch, src/mdmanager.cc:226-315), half drift.
+   Runs as CUDA graphs with device-side conditional rebuild nodes; nothing is
+   copied to the host. */
+mdg_status mdg_calculate(mdg_handle *h, int nsteps);
+
+/* Forces only, no kick (parity): f4 is n x 4, F = -dV/dq of the smoothed LJ
+   potential (the reference's kick with TimeStep = 1). */
+mdg_status mdg_forces(mdg_handle *h, double *f4);
+
+/* Replaces: KineticEnergyObserver, PotentialEnergyObserver, VirialObserver
+   (src/observer.cc:4-79) summed over the system as MDManager::ObserveDouble
+   does (src/mdmanager.cc:520-528): ke = sum 1/2 p^2, pe = sum of pair
+   energies, virial = sum(...)/3.  FP64 device reductions. */
+mdg_status mdg_observe(mdg_handle *h, double *ke, double *pe, double *virial);
+
+/* Pairlist readout for parity (MeshList::GetPairNumber, GetKeyPointer,
+   GetPartnerNumber, GetSortedList, include/meshlist.h:70-91).  Directed
+   (key, partner) pairs, expressed as upload indices, one per atom that has
+   the partner within SearchLength; *count returns the total, at most cap
+   entries are written. */
+mdg_status mdg_get_pairs(mdg_handle *h, int *key, int *partner, int64_t cap, int64_t *count);
+
+typedef struct {
+  int n;                  /* atoms */
+  int ncell[3];           /* cells per axis */
+  int max_neighbors;      /* neighbour-row capacity */
+  int max_row;            /* longest row of the last build */
+  int64_t list_entries;   /* entries of the last build (full list) */
+  int64_t steps;          /* MD steps taken */
+  int64_t rebuilds;       /* pairlist constructions (MeshList::GetNumberOfConstructions) */
+  int64_t displacement_checks;
+  double simulation_time;
+  double buffer_left;     /* skin budget (PairList::buffer_length) */
+} mdg_info;
+mdg_status mdg_get_info(mdg_handle *h, mdg_info *info);
+
+/* Device pointer of the handle's stream (cudaStream_t) and the handle's
+   internal timers: each call to mdg_calculate records CUDA events around
+   every force kernel when timing is on; mdg_kernel_time returns the summed
+   milliseconds and launch count of the force kernel since the last reset. */
+void *mdg_stream(mdg_handle *h);
+mdg_status mdg_set_kernel_timing(mdg_handle *h, int on);
+mdg_status mdg_kernel_time(mdg_handle *h, double *force_ms, int64_t *force_launches,
+                           int64_t *kernel_launches);
+
+const char *mdg_last_error(mdg_handle *h);
+const char *mdg_status_string(mdg_status s);
+/* Library version string. */
+const char *mdg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,337 @@
+"""mdacp_b200: B200-native Lennard-Jones timestep behind MDACP's interfaces.
+
+Python access to the C ABI of ``libmdacp_b200.so`` (declared in
+include/mdacp_b200.h) through ctypes.  The library is built in-tree by
+``__graft_entry__.build()`` (or ``make -C mdacp_b200/csrc``); importing this
+package never falls back to anything else: if the library is missing or no
+CUDA device is present, constructing a ``System`` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+import numpy as np
+
+__all__ = [
+    "LIB_PATH",
+    "MdgError",
+    "Params",
+    "Info",
+    "System",
+    "load_library",
+    "FP64",
+    "FP32_MIXED",
+    "NVE",
+    "NOSE_HOOVER",
+    "LANGEVIN",
+]
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "libmdacp_b200.so"
+
+FP64, FP32_MIXED = 0, 1
+NVE, NOSE_HOOVER, LANGEVIN = 0, 1, 2
+
+STATUS_NAMES = {
+    0: "MDG_OK",
+    -1: "MDG_ERR_INVALID_ARGUMENT",
+    -2: "MDG_ERR_CUDA",
+    -3: "MDG_ERR_CAPACITY",
+    -4: "MDG_ERR_TOO_FAST",
+    -5: "MDG_ERR_INVALID_POSITION",
+    -6: "MDG_ERR_NONFINITE",
+    -7: "MDG_ERR_BOX_TOO_SMALL",
+    -8: "MDG_ERR_TIMEOUT",
+    -9: "MDG_ERR_STATE",
+    -10: "MDG_ERR_NO_DEVICE",
+}
+
+
+class MdgError(RuntimeError):
+    """A non-zero mdg_status; ``status`` holds the code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Params(ctypes.Structure):
+    """``mdg_params`` (include/mdacp_b200.h)."""
+
+    _fields_ = [
+        ("capacity", ctypes.c_int),
+        ("L", ctypes.c_double * 3),
+        ("cutoff", ctypes.c_double),
+        ("buffer_length", ctypes.c_double),
+        ("time_step", ctypes.c_double),
+        ("precision", ctypes.c_int),
+        ("thermostat", ctypes.c_int),
+        ("aimed_temperature", ctypes.c_double),
+        ("heatbath_tau", ctypes.c_double),
+        ("heatbath_gamma", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+        ("check_list_length", ctypes.c_int),
+        ("max_neighbors", ctypes.c_int),
+        ("device", ctypes.c_int),
+        ("stream", ctypes.c_void_p),
+    ]
+
+
+class Info(ctypes.Structure):
+    """``mdg_info`` (include/mdacp_b200.h)."""
+
+    _fields_ = [
+        ("n", ctypes.c_int),
+        ("ncell", ctypes.c_int * 3),
+        ("max_neighbors", ctypes.c_int),
+        ("max_row", ctypes.c_int),
+        ("list_entries", ctypes.c_int64),
+        ("steps", ctypes.c_int64),
+        ("rebuilds", ctypes.c_int64),
+        ("displacement_checks", ctypes.c_int64),
+        ("simulation_time", ctypes.c_double),
+        ("buffer_left", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: (list(getattr(self, name)) if name == "ncell" else getattr(self, name))
+                for name, _ in self._fields_}
+
+
+# name -> (restype, argtypes)
+_H = ctypes.c_void_p
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+_I64P = ctypes.POINTER(ctypes.c_int64)
+SIGNATURES = {
+    "mdg_default_params": (None, [ctypes.POINTER(Params)]),
+    "mdg_create": (ctypes.c_int, [ctypes.POINTER(Params), ctypes.POINTER(_H)]),
+    "mdg_destroy": (ctypes.c_int, [_H]),
+    "mdg_set_state": (ctypes.c_int, [_H, _DP, _DP, _IP, ctypes.c_int]),
+    "mdg_get_state": (ctypes.c_int, [_H, _DP, _DP, _IP, ctypes.c_int]),
+    "mdg_get_ids": (ctypes.c_int, [_H, _IP, ctypes.c_int]),
+    "mdg_particle_number": (ctypes.c_int, [_H, _IP]),
+    "mdg_make_pairlist": (ctypes.c_int, [_H]),
+    "mdg_check_expired": (ctypes.c_int, [_H, _IP]),
+    "mdg_update_position_half": (ctypes.c_int, [_H]),
+    "mdg_calculate_force": (ctypes.c_int, [_H]),
+    "mdg_heatbath_zeta": (ctypes.c_int, [_H, ctypes.c_double]),
+    "mdg_heatbath_momenta": (ctypes.c_int, [_H]),
+    "mdg_langevin": (ctypes.c_int, [_H]),
+    "mdg_get_zeta": (ctypes.c_int, [_H, _DP]),
+    "mdg_set_zeta": (ctypes.c_int, [_H, ctypes.c_double]),
+    "mdg_calculate": (ctypes.c_int, [_H, ctypes.c_int]),
+    "mdg_forces": (ctypes.c_int, [_H, _DP]),
+    "mdg_observe": (ctypes.c_int, [_H, _DP, _DP, _DP]),
+    "mdg_get_pairs": (ctypes.c_int, [_H, _IP, _IP, ctypes.c_int64, _I64P]),
+    "mdg_get_info": (ctypes.c_int, [_H, ctypes.POINTER(Info)]),
+    "mdg_stream": (ctypes.c_void_p, [_H]),
+    "mdg_set_kernel_timing": (ctypes.c_int, [_H, ctypes.c_int]),
+    "mdg_kernel_time": (ctypes.c_int, [_H, _DP, _I64P, _I64P]),
+    "mdg_last_error": (ctypes.c_char_p, [_H]),
+    "mdg_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "mdg_version": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def load_library(path: pathlib.Path | None = None) -> ctypes.CDLL:
+    """Loads ``libmdacp_b200.so`` and declares every C-ABI signature; raises
+    if the library has not been built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = pathlib.Path(path or LIB_PATH)
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is not built; run __graft_entry__.build() or make -C mdacp_b200/csrc")
+    lib = ctypes.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_DP)
+
+
+def _i(a):
+    return a.ctypes.data_as(_IP)
+
+
+def _pad4(x: np.ndarray) -> np.ndarray:
+    out = np.zeros((x.shape[0], 4), dtype=np.float64)
+    out[:, :3] = x[:, :3]
+    return out
+
+
+class System:
+    """One handle: a periodic single-domain LJ system resident on a GPU."""
+
+    def __init__(self, L, cutoff=2.5, time_step=0.005, capacity=None, precision=FP64,
+                 thermostat=NVE, aimed_temperature=1.0, heatbath_tau=0.1, heatbath_gamma=0.1,
+                 seed=0, buffer_length=0.3, check_list_length=500, max_neighbors=0, device=0,
+                 stream=None, n_hint=None):
+        self.lib = load_library()
+        p = Params()
+        self.lib.mdg_default_params(ctypes.byref(p))
+        p.capacity = int(capacity or n_hint or 1)
+        p.L[:] = [float(x) for x in L]
+        p.cutoff = float(cutoff)
+        p.buffer_length = float(buffer_length)
+        p.time_step = float(time_step)
+        p.precision = int(precision)
+        p.thermostat = int(thermostat)
+        p.aimed_temperature = float(aimed_temperature)
+        p.heatbath_tau = float(heatbath_tau)
+        p.heatbath_gamma = float(heatbath_gamma)
+        p.seed = int(seed)
+        p.check_list_length = int(check_list_length)
+        p.max_neighbors = int(max_neighbors)
+        p.device = int(device)
+        p.stream = stream
+        self.params = p
+        h = _H()
+        st = self.lib.mdg_create(ctypes.byref(p), ctypes.byref(h))
+        if st != 0:
+            raise MdgError(st, self.lib.mdg_status_string(st).decode())
+        self.h = h
+        self.n = 0
+
+    # -- lifecycle
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mdg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st):
+        if st != 0:
+            msg = self.lib.mdg_last_error(self.h)
+            raise MdgError(st, (msg or b"").decode())
+
+    # -- state
+    def set_state(self, q, v, type_=None):
+        q4 = _pad4(np.asarray(q, dtype=np.float64))
+        v4 = _pad4(np.asarray(v, dtype=np.float64))
+        n = q4.shape[0]
+        t = None
+        if type_ is not None:
+            t = np.ascontiguousarray(type_, dtype=np.int32)
+        self._check(self.lib.mdg_set_state(self.h, _d(q4), _d(v4), _i(t) if t is not None else None, n))
+        self.n = n
+
+    def set_state4(self, q4, v4, type_=None):
+        """Uploads from caller-owned (n,4) float64 arrays without a copy."""
+        n = q4.shape[0]
+        t = _i(type_) if type_ is not None else None
+        self._check(self.lib.mdg_set_state(self.h, _d(q4), _d(v4), t, n))
+        self.n = n
+
+    def get_state4(self, q4, v4, type_=None):
+        t = _i(type_) if type_ is not None else None
+        self._check(self.lib.mdg_get_state(self.h, _d(q4), _d(v4), t, self.n))
+
+    def state(self):
+        """(q, v, ids) in the current slot order; ids are upload indices."""
+        q4 = np.empty((self.n, 4))
+        v4 = np.empty((self.n, 4))
+        self._check(self.lib.mdg_get_state(self.h, _d(q4), _d(v4), None, self.n))
+        return q4[:, :3].copy(), v4[:, :3].copy(), self.ids()
+
+    def state_by_id(self):
+        """(q, v) ordered by upload index."""
+        q, v, ids = self.state()
+        qo = np.empty_like(q)
+        vo = np.empty_like(v)
+        qo[ids] = q
+        vo[ids] = v
+        return qo, vo
+
+    def ids(self):
+        ids = np.empty(self.n, dtype=np.int32)
+        self._check(self.lib.mdg_get_ids(self.h, _i(ids), self.n))
+        return ids
+
+    # -- the hot path
+    def make_pairlist(self):
+        self._check(self.lib.mdg_make_pairlist(self.h))
+
+    def check_expired(self) -> bool:
+        e = ctypes.c_int()
+        self._check(self.lib.mdg_check_expired(self.h, ctypes.byref(e)))
+        return bool(e.value)
+
+    def update_position_half(self):
+        self._check(self.lib.mdg_update_position_half(self.h))
+
+    def calculate_force(self):
+        self._check(self.lib.mdg_calculate_force(self.h))
+
+    def calculate(self, nsteps: int = 1):
+        self._check(self.lib.mdg_calculate(self.h, int(nsteps)))
+
+    def forces(self):
+        """Forces in the current slot order."""
+        f4 = np.empty((self.n, 4))
+        self._check(self.lib.mdg_forces(self.h, _d(f4)))
+        return f4[:, :3].copy()
+
+    def forces_by_id(self):
+        f = self.forces()
+        out = np.empty_like(f)
+        out[self.ids()] = f
+        return out
+
+    def observe(self):
+        """(sum KE, sum PE, virial) as the reference's observers return them."""
+        ke, pe, vir = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mdg_observe(self.h, ctypes.byref(ke), ctypes.byref(pe), ctypes.byref(vir)))
+        return ke.value, pe.value, vir.value
+
+    def pairs(self):
+        """Directed (key, partner) pairs in upload indices."""
+        cnt = ctypes.c_int64()
+        self._check(self.lib.mdg_get_pairs(self.h, None, None, 0, ctypes.byref(cnt)))
+        k = np.empty(cnt.value, dtype=np.int32)
+        p = np.empty(cnt.value, dtype=np.int32)
+        self._check(self.lib.mdg_get_pairs(self.h, _i(k), _i(p), cnt.value, ctypes.byref(cnt)))
+        return k, p
+
+    def zeta(self) -> float:
+        z = ctypes.c_double()
+        self._check(self.lib.mdg_get_zeta(self.h, ctypes.byref(z)))
+        return z.value
+
+    def info(self) -> dict:
+        inf = Info()
+        self._check(self.lib.mdg_get_info(self.h, ctypes.byref(inf)))
+        return inf.as_dict()
+
+    def stream(self):
+        return self.lib.mdg_stream(self.h)
+
+    def set_kernel_timing(self, on: bool):
+        self._check(self.lib.mdg_set_kernel_timing(self.h, int(bool(on))))
+
+    def kernel_time(self):
+        ms = ctypes.c_double()
+        fl = ctypes.c_int64()
+        kl = ctypes.c_int64()
+        self._check(self.lib.mdg_kernel_time(self.h, ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(kl)))
+        return ms.value, fl.value, kl.value

@@ -1,0 +1,901 @@
+// C ABI of the B200 LJ timestep (include/mdacp_b200.h): handle, buffers,
+// the per-step kernel sequence and its CUDA-graph form with device-side
+// conditional nodes for the skin check and the pairlist rebuild.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mdacp_b200.h"
+#include "mdg_device.cuh"
+
+using namespace mdg;
+
+namespace {
+
+constexpr int kBlock = 256;       // streaming kernels
+constexpr int kForceBlock = 128;  // pair kernels
+constexpr int kStepsPerGraph = 20;
+
+int blocks_for(int n, int b) { return n > 0 ? (n + b - 1) / b : 1; }
+
+}  // namespace
+
+struct mdg_handle {
+  mdg_params prm{};
+  Box box{};
+  Arrays a{};
+  int n = 0;
+  int cap = 0;
+  int ncell = 0;
+  cudaStream_t stream = nullptr;      // work stream (user's or owned)
+  bool own_stream = false;
+  cudaStream_t cap_stream = nullptr;  // capture stream (always owned)
+  int *d_flags = nullptr;             // eager-mode conditional values
+  double *d_sums = nullptr;           // reduction outputs
+  size_t partial_cap = 0;
+  bool state_set = false;
+  // graph of kStepsPerGraph steps
+  cudaGraphExec_t exec = nullptr;
+  bool graph_dirty = true;
+  bool timing = false;
+  std::vector<cudaEvent_t> ev;        // force-kernel start/stop per step of the graph
+  double force_ms = 0.0;
+  int64_t force_launches = 0;
+  int64_t kernel_launches = 0;
+  int graph_kernel_count = 0;         // kernels per graph launch outside conditionals
+  std::string err;
+};
+
+namespace {
+
+mdg_status fail(mdg_handle *h, mdg_status s, const std::string &msg) {
+  if (h) h->err = msg;
+  return s;
+}
+
+#define CUDA_TRY(h, expr)                                                                  \
+  do {                                                                                     \
+    cudaError_t e_ = (expr);                                                               \
+    if (e_ != cudaSuccess) {                                                               \
+      return fail((h), MDG_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    }                                                                                      \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+  return cudaMalloc((void **)p, std::max<size_t>(count, 1) * sizeof(T));
+}
+
+void free_arrays(Arrays &a) {
+  void *ptrs[] = {a.q, a.v, a.q_old, a.qfix, a.ids, a.type, a.cell, a.nbr, a.nnbr, a.cell_count,
+                  a.cell_start, a.slot, a.perm, a.perm2, a.q_tmp, a.v_tmp, a.ids_tmp, a.type_tmp,
+                  a.cell_tmp, a.mult, a.cand, a.partials, a.st};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  a = Arrays{};
+}
+
+void destroy_graph(mdg_handle *h) {
+  if (h->exec) cudaGraphExecDestroy(h->exec);
+  h->exec = nullptr;
+  for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  h->ev.clear();
+  h->graph_dirty = true;
+}
+
+mdg_status translate_device_error(mdg_handle *h, const Status &st) {
+  if (st.error & kErrTooFast) {
+    char buf[160];
+    snprintf(buf, sizeof buf,
+             "Too fast particles exists. Try smaller time step (max_velocity = %g)", st.too_fast_v);
+    return fail(h, MDG_ERR_TOO_FAST, buf);
+  }
+  if (st.error & kErrNonFinite) return fail(h, MDG_ERR_NONFINITE, "non-finite position or velocity");
+  if (st.error & kErrInvalidPosition) return fail(h, MDG_ERR_INVALID_POSITION, "Invalid position");
+  if (st.error & kErrCapacity) return fail(h, MDG_ERR_CAPACITY, "neighbour capacity exceeded");
+  if (st.error & kErrTimeout) return fail(h, MDG_ERR_TIMEOUT, "device wait timed out");
+  return MDG_OK;
+}
+
+mdg_status read_status(mdg_handle *h, Status *st) {
+  CUDA_TRY(h, cudaMemcpyAsync(st, h->a.st, sizeof(Status), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return MDG_OK;
+}
+
+// (Re)allocates the neighbour table for `maxnb` partners per atom.
+mdg_status alloc_neighbors(mdg_handle *h, int maxnb) {
+  maxnb = std::max(8, (maxnb + 7) / 8 * 8);
+  if (h->a.nbr && maxnb <= h->a.maxnb) return MDG_OK;
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (h->a.nbr) cudaFree(h->a.nbr);
+  h->a.nbr = nullptr;
+  CUDA_TRY(h, dalloc(&h->a.nbr, (size_t)maxnb * h->a.stride));
+  h->a.maxnb = maxnb;
+  destroy_graph(h);
+  return MDG_OK;
+}
+
+// Neighbour-row capacity from the densest cell of the uploaded state.
+int estimate_max_neighbors(const mdg_handle *h, const double *q4, int n) {
+  const Box &b = h->box;
+  std::vector<int> count(h->ncell, 0);
+  int mx = 0;
+  for (int i = 0; i < n; i++) {
+    int c[3];
+    bool finite = true;
+    for (int d = 0; d < 3; d++) {
+      double x = q4[4 * i + d];
+      if (!std::isfinite(x)) {
+        finite = false;
+        break;
+      }
+      x -= b.L[d] * std::floor(x / b.L[d]);
+      const double k = std::floor(x * b.inv_cs[d]);
+      c[d] = k < 0.0 ? 0 : (k >= b.ms[d] ? b.ms[d] - 1 : (int)k);
+    }
+    if (!finite) continue;
+    const int idx = (c[2] * b.ms[1] + c[1]) * b.ms[0] + c[0];
+    mx = std::max(mx, ++count[idx]);
+  }
+  const double cell_vol = b.L[0] * b.L[1] * b.L[2] / (double)h->ncell;
+  const double rho_max = std::max((double)mx / cell_vol, (double)n / (b.L[0] * b.L[1] * b.L[2]));
+  const double sphere = 4.0 / 3.0 * M_PI * b.sl * b.sl * b.sl;
+  return (int)std::ceil(1.3 * rho_max * sphere + 24.0);
+}
+
+// ------------------------------------------------------ kernel sequences
+// Displacement check (PairList::CheckByDisplacement).
+void launch_disp(mdg_handle *h, cudaStream_t s) {
+  const int n = h->n;
+  k_disp_max<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(h->a, n);
+  k_disp_collect<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(h->a, h->box, n,
+                                                                   h->prm.check_list_length);
+  k_disp_pairs<1024><<<1, 1024, 0, s>>>(h->a, h->box);
+}
+
+// Pairlist rebuild (MDManager::MakePairList).
+void launch_build(mdg_handle *h, cudaStream_t s) {
+  const int n = h->n;
+  Arrays &a = h->a;
+  k_build_begin<<<1, 32, 0, s>>>(a);
+  cudaMemsetAsync(a.cell_count, 0, sizeof(int) * h->ncell, s);
+  k_cell_assign<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, h->box, n);
+  k_scan_cells<1024><<<1, 1024, 0, s>>>(a, h->ncell);
+  k_scatter<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, n);
+  k_sort_cells<<<blocks_for(h->ncell * 32, kBlock), kBlock, 0, s>>>(a, h->ncell);
+  k_permute<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, h->box, n);
+  cudaMemcpyAsync(a.q, a.q_tmp, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(a.v, a.v_tmp, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(a.ids, a.ids_tmp, sizeof(int) * n, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(a.type, a.type_tmp, sizeof(int) * n, cudaMemcpyDeviceToDevice, s);
+  k_build<kForceBlock><<<blocks_for(n, kForceBlock), kForceBlock, 0, s>>>(a, h->box, n);
+  k_build_done<<<1, 32, 0, s>>>(a, h->box);
+}
+
+template <int MODE>
+void launch_force_mode(mdg_handle *h, cudaStream_t s, const Thermo &th) {
+  const int n = h->n;
+  const int nb = blocks_for(n, kForceBlock);
+  if (h->prm.precision == MDG_FP32_MIXED)
+    k_force_fp32<kForceBlock, MODE><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th);
+  else
+    k_force_fp64<kForceBlock, MODE><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th);
+}
+
+Thermo thermo_of(const mdg_handle *h) {
+  Thermo th{};
+  th.gamma = h->prm.heatbath_gamma;
+  th.noise_sd = std::sqrt(2.0 * h->prm.heatbath_gamma * h->prm.aimed_temperature / h->prm.time_step);
+  th.seed = h->prm.seed;
+  return th;
+}
+
+void launch_drift(mdg_handle *h, cudaStream_t s, bool pack_fix, int track_vmax) {
+  const int nb = blocks_for(h->n, kBlock);
+  if (pack_fix)
+    k_drift<kBlock, true><<<nb, kBlock, 0, s>>>(h->a, h->box, h->n, track_vmax);
+  else
+    k_drift<kBlock, false><<<nb, kBlock, 0, s>>>(h->a, h->box, h->n, track_vmax);
+}
+
+// Everything of MDManager::Calculate after the rebuild decision; returns the
+// number of kernels launched.  ev_start/ev_stop bracket the force kernel.
+int launch_step_tail(mdg_handle *h, cudaStream_t s, cudaEvent_t ev_start, cudaEvent_t ev_stop,
+                     bool capture) {
+  const bool fix = h->prm.precision == MDG_FP32_MIXED;
+  const Thermo th = thermo_of(h);
+  const int n = h->n;
+  int launches = 0;
+  launch_drift(h, s, fix, 0);
+  launches++;
+  auto rec = [&](cudaEvent_t e) {
+    if (!e) return;
+    if (capture) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+    else cudaEventRecord(e, s);
+  };
+  if (h->prm.thermostat == MDG_NOSE_HOOVER) {
+    const int nbk = blocks_for(n, kBlock);
+    k_ke_partial<kBlock><<<nbk, kBlock, 0, s>>>(h->a, n);
+    k_zeta<1024><<<1, 1024, 0, s>>>(h->a, h->box, nbk, n, h->prm.aimed_temperature, h->prm.heatbath_tau);
+    rec(ev_start);
+    launch_force_mode<kKickNoseHoover>(h, s, th);
+    rec(ev_stop);
+    k_zeta<1024><<<1, 1024, 0, s>>>(h->a, h->box, blocks_for(n, kForceBlock), n,
+                                     h->prm.aimed_temperature, h->prm.heatbath_tau);
+    launch_drift(h, s, false, 1);
+    launches += 5;
+  } else if (h->prm.thermostat == MDG_LANGEVIN) {
+    rec(ev_start);
+    launch_force_mode<kKickLangevin>(h, s, th);
+    rec(ev_stop);
+    launches += 1;
+  } else {
+    rec(ev_start);
+    launch_force_mode<kKick>(h, s, th);
+    rec(ev_stop);
+    launch_drift(h, s, false, 1);
+    launches += 2;
+  }
+  k_step_done<<<1, 32, 0, s>>>(h->a, h->box);
+  return launches + 1;
+}
+
+// ---------------------------------------------------------- graph capture
+struct Capture {
+  cudaStream_t s;
+  cudaGraph_t g;
+  std::vector<cudaGraphNode_t> deps;
+};
+
+cudaError_t begin_capture(Capture &c) {
+  return cudaStreamBeginCaptureToGraph(c.s, c.g, c.deps.empty() ? nullptr : c.deps.data(), nullptr,
+                                       c.deps.size(), cudaStreamCaptureModeThreadLocal);
+}
+
+cudaError_t end_capture(Capture &c) {
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t *d = nullptr;
+  size_t nd = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(c.s, &cs, nullptr, nullptr, &d, &nd);
+  if (e != cudaSuccess) return e;
+  std::vector<cudaGraphNode_t> frontier(d, d + nd);
+  cudaGraph_t out = nullptr;
+  e = cudaStreamEndCapture(c.s, &out);
+  if (e != cudaSuccess) return e;
+  if (!frontier.empty()) c.deps = frontier;
+  return cudaSuccess;
+}
+
+// Appends an IF node on `h_cond` after the current frontier; returns its body.
+cudaError_t add_if(Capture &c, cudaGraphConditionalHandle hc, cudaGraph_t *body) {
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = hc;
+  p.conditional.type = cudaGraphCondTypeIf;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  cudaError_t e = cudaGraphAddNode(&node, c.g, c.deps.empty() ? nullptr : c.deps.data(),
+                                   c.deps.size(), &p);
+  if (e != cudaSuccess) return e;
+  *body = p.conditional.phGraph_out[0];
+  c.deps.assign(1, node);
+  return cudaSuccess;
+}
+
+mdg_status build_graph(mdg_handle *h) {
+  destroy_graph(h);
+  cudaGraph_t g;
+  CUDA_TRY(h, cudaGraphCreate(&g, 0));
+  if (h->timing) {
+    h->ev.resize(2 * kStepsPerGraph);
+    for (auto &e : h->ev) CUDA_TRY(h, cudaEventCreate(&e));
+  }
+  Capture c{h->cap_stream, g, {}};
+  int kernels = 0;
+  for (int s = 0; s < kStepsPerGraph; s++) {
+    cudaGraphConditionalHandle hd, hb;
+    CUDA_TRY(h, cudaGraphConditionalHandleCreate(&hd, g, 0, cudaGraphCondAssignDefault));
+    CUDA_TRY(h, cudaGraphConditionalHandleCreate(&hb, g, 0, cudaGraphCondAssignDefault));
+    CUDA_TRY(h, begin_capture(c));
+    k_expiry<<<1, 32, 0, c.s>>>(h->a, h->box, hd, 1, h->d_flags);
+    CUDA_TRY(h, end_capture(c));
+    cudaGraph_t body;
+    CUDA_TRY(h, add_if(c, hd, &body));
+    {
+      Capture bc{h->cap_stream, body, {}};
+      CUDA_TRY(h, begin_capture(bc));
+      launch_disp(h, bc.s);
+      CUDA_TRY(h, end_capture(bc));
+    }
+    CUDA_TRY(h, begin_capture(c));
+    k_decide<<<1, 32, 0, c.s>>>(h->a, hb, 1, h->d_flags);
+    CUDA_TRY(h, end_capture(c));
+    CUDA_TRY(h, add_if(c, hb, &body));
+    {
+      Capture bc{h->cap_stream, body, {}};
+      CUDA_TRY(h, begin_capture(bc));
+      launch_build(h, bc.s);
+      CUDA_TRY(h, end_capture(bc));
+    }
+    CUDA_TRY(h, begin_capture(c));
+    kernels += 2 + launch_step_tail(h, c.s, h->timing ? h->ev[2 * s] : nullptr,
+                                    h->timing ? h->ev[2 * s + 1] : nullptr, true);
+    CUDA_TRY(h, end_capture(c));
+  }
+  cudaError_t e = cudaGraphInstantiate(&h->exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(h, MDG_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  h->graph_kernel_count = kernels;
+  h->graph_dirty = false;
+  return MDG_OK;
+}
+
+// One step with host-side decisions (used for partial chunks and by the
+// fine-grained entry points).
+mdg_status step_eager(mdg_handle *h) {
+  int flags[2] = {0, 0};
+  k_expiry<<<1, 32, 0, h->stream>>>(h->a, h->box, 0, 0, h->d_flags);
+  CUDA_TRY(h, cudaMemcpyAsync(flags, h->d_flags, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  h->kernel_launches++;
+  if (flags[0]) {
+    launch_disp(h, h->stream);
+    h->kernel_launches += 3;
+  }
+  k_decide<<<1, 32, 0, h->stream>>>(h->a, 0, 0, h->d_flags);
+  CUDA_TRY(h, cudaMemcpyAsync(flags, h->d_flags, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  h->kernel_launches++;
+  if (flags[1]) {
+    launch_build(h, h->stream);
+    h->kernel_launches += 9;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (h->timing) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+  }
+  h->kernel_launches += launch_step_tail(h, h->stream, e0, e1, false);
+  CUDA_TRY(h, cudaGetLastError());
+  if (h->timing) {
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    h->force_ms += ms;
+    h->force_launches++;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  return MDG_OK;
+}
+
+mdg_status check_ready(mdg_handle *h) {
+  if (!h) return MDG_ERR_INVALID_ARGUMENT;
+  if (!h->state_set) return fail(h, MDG_ERR_STATE, "no state uploaded (mdg_set_state)");
+  return MDG_OK;
+}
+
+// Builds the list now if it is stale (forces / observers need a valid list).
+mdg_status ensure_list(mdg_handle *h) {
+  Status st;
+  mdg_status r = read_status(h, &st);
+  if (r) return r;
+  if (st.error) return translate_device_error(h, st);
+  if (!st.list_stale) return MDG_OK;
+  for (int attempt = 0; attempt < 4; attempt++) {
+    launch_build(h, h->stream);
+    h->kernel_launches += 9;
+    CUDA_TRY(h, cudaGetLastError());
+    r = read_status(h, &st);
+    if (r) return r;
+    if (!(st.error & kErrCapacity)) break;
+    // grow the rows and build again
+    r = alloc_neighbors(h, (int)(st.max_row * 1.25) + 8);
+    if (r) return r;
+    const int zero = 0, one = 1;
+    CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->error, &zero, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->list_stale, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  }
+  if (st.error) return translate_device_error(h, st);
+  return MDG_OK;
+}
+
+}  // namespace
+
+// ================================================================== C ABI
+extern "C" {
+
+void mdg_default_params(mdg_params *p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->capacity = 1000000;
+  p->L[0] = p->L[1] = p->L[2] = 10.0;
+  p->cutoff = 3.0;             // CUTOFF_LENGTH, include/mdconfig.h:31
+  p->buffer_length = 0.3;      // src/simulationinfo.cc:6
+  p->time_step = 0.001;        // src/simulationinfo.cc:9
+  p->precision = MDG_FP64;
+  p->thermostat = MDG_NVE;
+  p->aimed_temperature = 1.0;  // src/simulationinfo.cc:11
+  p->heatbath_tau = 0.1;       // src/simulationinfo.cc:13
+  p->heatbath_gamma = 0.1;     // src/simulationinfo.cc:14
+  p->seed = 0;
+  p->check_list_length = 500;  // src/simulationinfo.cc:28
+  p->max_neighbors = 0;
+  p->device = 0;
+  p->stream = nullptr;
+}
+
+mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
+  if (!prm || !out) return MDG_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (prm->capacity < 1 || prm->cutoff <= 0.0 || prm->buffer_length < 0.0 || prm->time_step <= 0.0 ||
+      prm->check_list_length < 1 || (prm->precision != MDG_FP64 && prm->precision != MDG_FP32_MIXED) ||
+      prm->thermostat < MDG_NVE || prm->thermostat > MDG_LANGEVIN)
+    return MDG_ERR_INVALID_ARGUMENT;
+  for (int d = 0; d < 3; d++)
+    if (!(prm->L[d] > 0.0) || !std::isfinite(prm->L[d])) return MDG_ERR_INVALID_ARGUMENT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MDG_ERR_NO_DEVICE;
+  if (prm->device < 0 || prm->device >= ndev) return MDG_ERR_INVALID_ARGUMENT;
+
+  mdg_handle *h = new mdg_handle();
+  h->prm = *prm;
+  Box &b = h->box;
+  const double SL = prm->cutoff + prm->buffer_length;  // src/simulationinfo.cc:6-7
+  for (int d = 0; d < 3; d++) {
+    b.L[d] = prm->L[d];
+    b.hL[d] = 0.5 * prm->L[d];
+    b.ms[d] = (int)(prm->L[d] / SL);  // MeshList::ChangeScale, src/meshlist.cc:50-52
+    if (b.ms[d] < 3) {
+      delete h;
+      return MDG_ERR_BOX_TOO_SMALL;
+    }
+    b.inv_cs[d] = (double)b.ms[d] / prm->L[d];
+    b.fix_scale[d] = (float)(prm->L[d] / 4294967296.0);
+  }
+  b.ncell = b.ms[0] * b.ms[1] * b.ms[2];
+  b.sl = SL;
+  b.sl2 = SL * SL;
+  b.rc2 = prm->cutoff * prm->cutoff;
+  {  // Variables::Variables, src/variables.cc:21-27
+    const double s2 = 1.0 / (prm->cutoff * prm->cutoff);
+    const double s6 = s2 * s2 * s2, s8 = s6 * s2, s12 = s6 * s6, s14 = s12 * s2;
+    b.c2 = 6.0 * s14 - 3.0 * s8;
+    b.c0 = -s12 + s6 - b.c2 / s2;
+  }
+  b.dt = prm->time_step;
+  b.buffer_length = prm->buffer_length;
+  b.rc2f = (float)b.rc2;
+  b.c2x8f = (float)(b.c2 * 8.0);
+  b.check_list_length = prm->check_list_length;
+  h->ncell = b.ncell;
+  h->cap = prm->capacity;
+
+  cudaError_t e = cudaSetDevice(prm->device);
+  if (e == cudaSuccess) {
+    if (prm->stream) {
+      h->stream = (cudaStream_t)prm->stream;
+    } else {
+      e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+      h->own_stream = true;
+    }
+  }
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
+  Arrays &a = h->a;
+  const int cap = h->cap;
+  a.stride = (cap + 31) / 32 * 32;
+  a.maxnb = 0;
+  h->partial_cap = (size_t)blocks_for(cap, kForceBlock) * 3 + 64;
+  if (e == cudaSuccess) e = dalloc(&a.q, cap);
+  if (e == cudaSuccess) e = dalloc(&a.v, cap);
+  if (e == cudaSuccess) e = dalloc(&a.q_old, cap);
+  if (e == cudaSuccess) e = dalloc(&a.qfix, cap);
+  if (e == cudaSuccess) e = dalloc(&a.ids, cap);
+  if (e == cudaSuccess) e = dalloc(&a.type, cap);
+  if (e == cudaSuccess) e = dalloc(&a.cell, cap);
+  if (e == cudaSuccess) e = dalloc(&a.nnbr, cap);
+  if (e == cudaSuccess) e = dalloc(&a.cell_count, b.ncell);
+  if (e == cudaSuccess) e = dalloc(&a.cell_start, b.ncell + 1);
+  if (e == cudaSuccess) e = dalloc(&a.slot, cap);
+  if (e == cudaSuccess) e = dalloc(&a.perm, cap);
+  if (e == cudaSuccess) e = dalloc(&a.perm2, cap);
+  if (e == cudaSuccess) e = dalloc(&a.q_tmp, cap);
+  if (e == cudaSuccess) e = dalloc(&a.v_tmp, cap);
+  if (e == cudaSuccess) e = dalloc(&a.ids_tmp, cap);
+  if (e == cudaSuccess) e = dalloc(&a.type_tmp, cap);
+  if (e == cudaSuccess) e = dalloc(&a.cell_tmp, cap);
+  if (e == cudaSuccess) e = dalloc(&a.mult, cap);
+  if (e == cudaSuccess) e = dalloc(&a.cand, prm->check_list_length);
+  if (e == cudaSuccess) e = dalloc(&a.partials, h->partial_cap);
+  if (e == cudaSuccess) e = dalloc(&a.st, 1);
+  if (e == cudaSuccess) e = dalloc(&h->d_flags, 4);
+  if (e == cudaSuccess) e = dalloc(&h->d_sums, 8);
+  if (e == cudaSuccess) e = cudaMemsetAsync(a.st, 0, sizeof(Status), h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    free_arrays(a);
+    delete h;
+    return MDG_ERR_CUDA;
+  }
+  if (prm->max_neighbors > 0) {
+    mdg_status r = alloc_neighbors(h, prm->max_neighbors);
+    if (r) {
+      free_arrays(a);
+      delete h;
+      return r;
+    }
+  }
+  *out = h;
+  return MDG_OK;
+}
+
+mdg_status mdg_destroy(mdg_handle *h) {
+  if (!h) return MDG_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(h->prm.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  destroy_graph(h);
+  free_arrays(h->a);
+  if (h->d_flags) cudaFree(h->d_flags);
+  if (h->d_sums) cudaFree(h->d_sums);
+  if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return MDG_OK;
+}
+
+mdg_status mdg_set_state(mdg_handle *h, const double *q4, const double *v4, const int *type, int n) {
+  if (!h || n < 0 || (n > 0 && (!q4 || !v4))) return MDG_ERR_INVALID_ARGUMENT;
+  if (n > h->cap) return fail(h, MDG_ERR_CAPACITY, "more atoms than the handle's capacity");
+  CUDA_TRY(h, cudaSetDevice(h->prm.device));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (n > 0) {
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.q, q4, sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.v, v4, sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
+    std::vector<int> ids(n), ty(n, 0);
+    for (int i = 0; i < n; i++) ids[i] = i;
+    if (type) std::copy(type, type + n, ty.begin());
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.ids, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.type, ty.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    if (h->prm.max_neighbors <= 0 && (!h->a.nbr || n != h->n)) {
+      mdg_status r = alloc_neighbors(h, estimate_max_neighbors(h, q4, n));
+      if (r) return r;
+    }
+  } else if (!h->a.nbr) {
+    mdg_status r = alloc_neighbors(h, 8);
+    if (r) return r;
+  }
+  // fresh bookkeeping; keep counters of steps / rebuilds / time / zeta
+  Status st;
+  mdg_status r = read_status(h, &st);
+  if (r) return r;
+  st.error = 0;
+  st.list_stale = 1;
+  st.vmax2_bits = 0;
+  st.budget = h->prm.buffer_length;
+  CUDA_TRY(h, cudaMemcpyAsync(h->a.st, &st, sizeof(Status), cudaMemcpyHostToDevice, h->stream));
+  if (n > 0) k_vmax<kBlock><<<blocks_for(n, kBlock), kBlock, 0, h->stream>>>(h->a, n);
+  CUDA_TRY(h, cudaGetLastError());
+  if (n != h->n) h->graph_dirty = true;
+  h->n = n;
+  int dev_error = 0;
+  CUDA_TRY(h, cudaMemcpyAsync(&dev_error, &h->a.st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (dev_error) {
+    h->state_set = false;
+    const int zero = 0;
+    CUDA_TRY(h, cudaMemcpy(&h->a.st->error, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    return fail(h, MDG_ERR_NONFINITE, "non-finite value in the uploaded state");
+  }
+  h->state_set = true;
+  return MDG_OK;
+}
+
+mdg_status mdg_get_state(mdg_handle *h, double *q4, double *v4, int *type, int n) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (n != h->n) return fail(h, MDG_ERR_INVALID_ARGUMENT, "n differs from the handle's atom count");
+  if (n == 0) return MDG_OK;
+  if (q4) CUDA_TRY(h, cudaMemcpyAsync(q4, h->a.q, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
+  if (v4) CUDA_TRY(h, cudaMemcpyAsync(v4, h->a.v, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
+  if (type) CUDA_TRY(h, cudaMemcpyAsync(type, h->a.type, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return MDG_OK;
+}
+
+mdg_status mdg_get_ids(mdg_handle *h, int *ids, int n) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (n != h->n || (n > 0 && !ids)) return fail(h, MDG_ERR_INVALID_ARGUMENT, "bad ids buffer");
+  if (n == 0) return MDG_OK;
+  CUDA_TRY(h, cudaMemcpyAsync(ids, h->a.ids, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return MDG_OK;
+}
+
+mdg_status mdg_particle_number(mdg_handle *h, int *n) {
+  if (!h || !n) return MDG_ERR_INVALID_ARGUMENT;
+  *n = h->n;
+  return MDG_OK;
+}
+
+mdg_status mdg_make_pairlist(mdg_handle *h) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (h->n == 0) return MDG_OK;
+  const int one = 1;
+  CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->list_stale, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  return ensure_list(h);
+}
+
+mdg_status mdg_check_expired(mdg_handle *h, int *expired) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (!expired) return MDG_ERR_INVALID_ARGUMENT;
+  *expired = 0;
+  if (h->n == 0) return MDG_OK;
+  k_vmax<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->n);
+  int flags[2] = {0, 0};
+  k_expiry<<<1, 32, 0, h->stream>>>(h->a, h->box, 0, 0, h->d_flags);
+  CUDA_TRY(h, cudaMemcpyAsync(flags, h->d_flags, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (flags[0]) launch_disp(h, h->stream);
+  k_decide<<<1, 32, 0, h->stream>>>(h->a, 0, 0, h->d_flags);
+  CUDA_TRY(h, cudaMemcpyAsync(flags, h->d_flags, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  Status st;
+  r = read_status(h, &st);
+  if (r) return r;
+  if (st.error) return translate_device_error(h, st);
+  *expired = flags[1];
+  return MDG_OK;
+}
+
+mdg_status mdg_update_position_half(mdg_handle *h) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (h->n == 0) return MDG_OK;
+  launch_drift(h, h->stream, h->prm.precision == MDG_FP32_MIXED, 0);
+  CUDA_TRY(h, cudaGetLastError());
+  return MDG_OK;
+}
+
+mdg_status mdg_calculate_force(mdg_handle *h) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (h->n == 0) return MDG_OK;
+  if ((r = ensure_list(h))) return r;
+  if (h->prm.precision == MDG_FP32_MIXED)
+    k_pack_fix<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n);
+  launch_force_mode<kKick>(h, h->stream, thermo_of(h));
+  CUDA_TRY(h, cudaGetLastError());
+  return MDG_OK;
+}
+
+mdg_status mdg_heatbath_zeta(mdg_handle *h, double t) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  Status st;
+  if ((r = read_status(h, &st))) return r;
+  const double dt2 = h->prm.time_step * 0.5;
+  const double tau = h->prm.heatbath_tau;
+  st.zeta += (t - h->prm.aimed_temperature) / (tau * tau) * dt2;
+  CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->zeta, &st.zeta, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return MDG_OK;
+}
+
+mdg_status mdg_heatbath_momenta(mdg_handle *h) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (h->n == 0) return MDG_OK;
+  k_scale_v<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->n, h->prm.time_step * 0.5);
+  CUDA_TRY(h, cudaGetLastError());
+  return MDG_OK;
+}
+
+mdg_status mdg_langevin(mdg_handle *h) {
+  // The Langevin update is fused into the force kick of mdg_calculate; alone
+  // it needs a kick of zero force, which is what a force-free step is not:
+  // expose it only through the full step.
+  return fail(h, MDG_ERR_STATE, "mdg_langevin: use mdg_calculate with thermostat MDG_LANGEVIN");
+}
+
+mdg_status mdg_get_zeta(mdg_handle *h, double *zeta) {
+  if (!h || !zeta) return MDG_ERR_INVALID_ARGUMENT;
+  Status st;
+  mdg_status r = read_status(h, &st);
+  if (r) return r;
+  *zeta = st.zeta;
+  return MDG_OK;
+}
+
+mdg_status mdg_set_zeta(mdg_handle *h, double zeta) {
+  if (!h) return MDG_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->zeta, &zeta, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return MDG_OK;
+}
+
+mdg_status mdg_calculate(mdg_handle *h, int nsteps) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (nsteps < 0) return MDG_ERR_INVALID_ARGUMENT;
+  if (h->n == 0 || nsteps == 0) return MDG_OK;
+  CUDA_TRY(h, cudaSetDevice(h->prm.device));
+  Status st;
+  if ((r = read_status(h, &st))) return r;
+  if (st.error) return translate_device_error(h, st);
+  long long target = st.steps + nsteps;
+  for (int attempt = 0; attempt < 8; attempt++) {
+    long long left = target - st.steps;
+    if (left <= 0) break;
+    if (left >= kStepsPerGraph && h->graph_dirty) {
+      if ((r = build_graph(h))) return r;
+    }
+    while (left >= kStepsPerGraph) {
+      CUDA_TRY(h, cudaGraphLaunch(h->exec, h->stream));
+      h->kernel_launches += h->graph_kernel_count;
+      left -= kStepsPerGraph;
+      if (h->timing) {
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        for (int s = 0; s < kStepsPerGraph; s++) {
+          float ms = 0.f;
+          CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev[2 * s], h->ev[2 * s + 1]));
+          h->force_ms += ms;
+          h->force_launches++;
+        }
+      }
+    }
+    while (left > 0) {
+      if ((r = step_eager(h))) return r;
+      left--;
+    }
+    if ((r = read_status(h, &st))) return r;
+    if (st.error == kErrCapacity) {
+      // a rebuild overflowed a neighbour row: grow, rebuild, redo the rest
+      if ((r = alloc_neighbors(h, (int)(st.max_row * 1.25) + 8))) return r;
+      st.error = 0;
+      st.list_stale = 1;
+      CUDA_TRY(h, cudaMemcpyAsync(h->a.st, &st, sizeof(Status), cudaMemcpyHostToDevice, h->stream));
+      continue;
+    }
+    if (st.error) return translate_device_error(h, st);
+  }
+  if (st.steps < target) return fail(h, MDG_ERR_CAPACITY, "could not complete the steps");
+  return MDG_OK;
+}
+
+mdg_status mdg_forces(mdg_handle *h, double *f4) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (h->n == 0) return MDG_OK;
+  if (!f4) return MDG_ERR_INVALID_ARGUMENT;
+  if ((r = ensure_list(h))) return r;
+  if (h->prm.precision == MDG_FP32_MIXED)
+    k_pack_fix<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n);
+  launch_force_mode<kForceOut>(h, h->stream, thermo_of(h));
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaMemcpyAsync(f4, h->a.v_tmp, sizeof(double4) * h->n, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return MDG_OK;
+}
+
+mdg_status mdg_observe(mdg_handle *h, double *ke, double *pe, double *virial) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  double out[3] = {0.0, 0.0, 0.0};
+  if (h->n > 0) {
+    if ((r = ensure_list(h))) return r;
+    const int nb = blocks_for(h->n, kBlock);
+    k_observe<kBlock><<<nb, kBlock, 0, h->stream>>>(h->a, h->box, h->n);
+    k_final_sum<256, 3><<<1, 256, 0, h->stream>>>(h->a.partials, nb, h->d_sums);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemcpyAsync(out, h->d_sums, sizeof out, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  }
+  if (ke) *ke = out[0];
+  if (pe) *pe = out[1];
+  if (virial) *virial = out[2] / 3.0;
+  return MDG_OK;
+}
+
+mdg_status mdg_get_pairs(mdg_handle *h, int *key, int *partner, int64_t cap, int64_t *count) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (!count || cap < 0) return MDG_ERR_INVALID_ARGUMENT;
+  *count = 0;
+  if (h->n == 0) return MDG_OK;
+  if ((r = ensure_list(h))) return r;
+  const int n = h->n, stride = h->a.stride;
+  std::vector<int> nn(n), ids(n);
+  CUDA_TRY(h, cudaMemcpyAsync(nn.data(), h->a.nnbr, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(ids.data(), h->a.ids, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  const int maxrow = n > 0 ? *std::max_element(nn.begin(), nn.end()) : 0;
+  std::vector<int> tab((size_t)maxrow * stride);
+  if (maxrow > 0)
+    CUDA_TRY(h, cudaMemcpy(tab.data(), h->a.nbr, sizeof(int) * (size_t)maxrow * stride, cudaMemcpyDeviceToHost));
+  int64_t c = 0;
+  for (int i = 0; i < n; i++) {
+    for (int k = 0; k < nn[i]; k++) {
+      if (c < cap && key && partner) {
+        key[c] = ids[i];
+        partner[c] = ids[tab[(size_t)k * stride + i]];
+      }
+      c++;
+    }
+  }
+  *count = c;
+  return MDG_OK;
+}
+
+mdg_status mdg_get_info(mdg_handle *h, mdg_info *info) {
+  if (!h || !info) return MDG_ERR_INVALID_ARGUMENT;
+  Status st;
+  mdg_status r = read_status(h, &st);
+  if (r) return r;
+  info->n = h->n;
+  for (int d = 0; d < 3; d++) info->ncell[d] = h->box.ms[d];
+  info->max_neighbors = h->a.maxnb;
+  info->max_row = st.max_row;
+  info->list_entries = st.list_entries;
+  info->steps = st.steps;
+  info->rebuilds = st.rebuilds;
+  info->displacement_checks = st.disp_checks;
+  info->simulation_time = st.sim_time;
+  info->buffer_left = st.budget;
+  return MDG_OK;
+}
+
+void *mdg_stream(mdg_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+mdg_status mdg_set_kernel_timing(mdg_handle *h, int on) {
+  if (!h) return MDG_ERR_INVALID_ARGUMENT;
+  if ((on != 0) != h->timing) {
+    h->timing = on != 0;
+    destroy_graph(h);
+  }
+  h->force_ms = 0.0;
+  h->force_launches = 0;
+  h->kernel_launches = 0;
+  return MDG_OK;
+}
+
+mdg_status mdg_kernel_time(mdg_handle *h, double *force_ms, int64_t *force_launches,
+                           int64_t *kernel_launches) {
+  if (!h) return MDG_ERR_INVALID_ARGUMENT;
+  if (force_ms) *force_ms = h->force_ms;
+  if (force_launches) *force_launches = h->force_launches;
+  if (kernel_launches) *kernel_launches = h->kernel_launches;
+  return MDG_OK;
+}
+
+const char *mdg_last_error(mdg_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+const char *mdg_status_string(mdg_status s) {
+  switch (s) {
+    case MDG_OK: return "ok";
+    case MDG_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case MDG_ERR_CUDA: return "CUDA error";
+    case MDG_ERR_CAPACITY: return "capacity exceeded";
+    case MDG_ERR_TOO_FAST: return "too fast particle";
+    case MDG_ERR_INVALID_POSITION: return "invalid position";
+    case MDG_ERR_NONFINITE: return "non-finite state";
+    case MDG_ERR_BOX_TOO_SMALL: return "box too small for the cell list";
+    case MDG_ERR_TIMEOUT: return "device wait timed out";
+    case MDG_ERR_STATE: return "call out of order";
+    case MDG_ERR_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+const char *mdg_version(void) { return "mdacp_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,821 @@
+// Device code of the B200 LJ timestep: cell sort, Verlet list build, force
+// kick (FP64 drop-in and FP32-mixed), drift, skin bookkeeping, thermostats
+// and FP64 observables.  Host orchestration lives in mdg_api.cu.
+//
+// Data layout in HBM (n atoms, slots renumbered in cell order at every
+// rebuild):
+//   q, v      double4[cap]   position (unwrapped between rebuilds), velocity
+//   qfix      int4[cap]      fixed-point copy of q for the FP32-mixed force:
+//                            x_fix = round(frac(x/L) * 2^32) as uint32, so the
+//                            int32 difference of two atoms is the minimum-image
+//                            displacement in units of L/2^32 (no shift tables)
+//   nbr       int32[maxnb][stride]  full Verlet list, column-major: entry k
+//                            of atom i at nbr[k*stride + i] (coalesced per warp)
+//   nnbr      int32[cap]     row lengths
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mdg {
+
+constexpr int kErrCapacity = 1;
+constexpr int kErrTooFast = 2;
+constexpr int kErrInvalidPosition = 4;
+constexpr int kErrNonFinite = 8;
+constexpr int kErrTimeout = 16;
+
+// Geometry and force constants, passed by value to every kernel.
+struct Box {
+  double L[3];
+  double hL[3];        // L/2, minimum-image threshold
+  double inv_cs[3];    // 1 / cell size
+  int ms[3];           // cells per axis (MeshList::ChangeScale: int(L/SL))
+  int ncell;
+  double sl;           // SearchLength
+  double sl2;          // SearchLength^2
+  double rc2;          // CUTOFF_LENGTH^2
+  double c0, c2;       // smoothed-LJ constants (Variables::C0, C2)
+  double dt;           // TimeStep
+  double buffer_length;
+  float fix_scale[3];  // L / 2^32
+  float rc2f;
+  float c2x8f;
+  int check_list_length;
+};
+
+// Mutable device-side state of one handle.
+struct Status {
+  int error;                        // kErr* flags; any set flag halts the step kernels
+  int list_stale;                   // 1: next step rebuilds unconditionally
+  unsigned long long vmax2_bits;    // max |v|^2 of the last velocity update (double bits)
+  double budget;                    // PairList::buffer_length
+  unsigned long long dr2max_bits;   // displacement check: max |dq|^2
+  int cand_weighted;                // candidates counted with their image multiplicity
+  int cand_n;                       // candidate atoms stored
+  int max_row;                      // longest neighbour row of the last build
+  int want_build;                   // this step rebuilds the list
+  long long list_entries;
+  long long total_images;           // real atoms + ghost images (PairList Nl bound)
+  long long rebuilds;
+  long long steps;
+  long long disp_checks;
+  double zeta;                      // Nose-Hoover friction (Variables::Zeta)
+  double sim_time;
+  double too_fast_v;                // speed that tripped kErrTooFast
+};
+
+struct Arrays {
+  double4 *q, *v, *q_old;
+  int4 *qfix;
+  int *ids, *type;
+  int *cell;          // cell of each slot at the last build
+  int *nbr, *nnbr;
+  int *cell_count, *cell_start;
+  int *slot;          // rank inside the cell from the atomic scatter
+  int *perm, *perm2;  // new slot -> old slot
+  double4 *q_tmp, *v_tmp;
+  int *ids_tmp, *type_tmp, *cell_tmp;
+  unsigned char *mult; // image multiplicity at the last build (1..27)
+  int *cand;          // displacement-check candidates
+  double *partials;   // per-block partial sums for reductions
+  Status *st;
+  int stride;         // column stride of nbr (>= cap, multiple of 32)
+  int maxnb;          // neighbour-row capacity
+};
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+__device__ __forceinline__ void atomic_max_double_bits(unsigned long long *addr, double v) {
+  // non-negative doubles order like their bit patterns
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide max of a non-negative double, one atomic per block.
+template <int BLOCK>
+__device__ __forceinline__ void block_max_to(unsigned long long *addr, double v) {
+  __shared__ double sm[BLOCK / 32];
+  v = warp_max(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sm[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < BLOCK / 32) ? sm[l] : 0.0;
+    v = warp_max(v);
+    if (l == 0) atomic_max_double_bits(addr, v);
+  }
+}
+
+// Fixed order block sum written to partials[blockIdx.x * nsum + k].
+template <int BLOCK, int NSUM>
+__device__ __forceinline__ void block_sum_to(double (&v)[NSUM], double *partials) {
+  __shared__ double sm[NSUM][BLOCK / 32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < NSUM; k++) {
+    double x = warp_sum(v[k]);
+    if (l == 0) sm[k][w] = x;
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < NSUM; k++) {
+      double x = (l < BLOCK / 32) ? sm[k][l] : 0.0;
+      x = warp_sum(x);
+      if (l == 0) partials[(size_t)blockIdx.x * NSUM + k] = x;
+    }
+  }
+}
+
+__device__ __forceinline__ int cell_coord(double x, double inv_cs, int ms) {
+  int c = (int)(x * inv_cs);
+  return c < 0 ? 0 : (c >= ms ? ms - 1 : c);
+}
+
+// Fixed-point image of one coordinate: frac(x / L) * 2^32 rounded, mod 2^32.
+__device__ __forceinline__ int fixed_coord(double x, double L) {
+  double u = x / L;
+  u -= floor(u);
+  const long long k = __double2ll_rn(u * 4294967296.0);
+  return (int)(unsigned int)(unsigned long long)k;
+}
+
+// Minimum-image ghost coordinate as the reference forms it: the copy of
+// atom j that lies next to atom i is q_j + diff with diff in {-L, 0, +L}
+// (MDUnit::MakeBufferForBorderParticles, src/mdunit.cc:152-192).
+__device__ __forceinline__ double image_of(double xj, double xi, double L, double hL) {
+  const double t = xj - xi;
+  if (t > hL) return dsub(xj, L);
+  if (t < -hL) return dadd(xj, L);
+  return xj;
+}
+
+// ---------------------------------------------------------------- kernels
+// Initial |v|^2 maximum (used before the first step after an upload) and a
+// finiteness check of the uploaded state.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_vmax(Arrays a, int n) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  double v2 = 0.0;
+  if (i < n) {
+    const double4 v = a.v[i];
+    const double4 q = a.q[i];
+    v2 = dadd(dadd(dmul(v.x, v.x), dmul(v.y, v.y)), dmul(v.z, v.z));
+    if (!isfinite(v2) || !isfinite(q.x) || !isfinite(q.y) || !isfinite(q.z)) {
+      atomicOr(&a.st->error, kErrNonFinite);
+      v2 = 0.0;
+    }
+  }
+  block_max_to<BLOCK>(&a.st->vmax2_bits, v2);
+}
+
+// PairList::IsPairListExpired (src/pairlist.cc:25-65): budget -= 2 vmax dt
+// while the budget is positive (a too-fast atom is an error), then arm the
+// displacement check once the budget is spent.  Sets the two conditional
+// handles of this step's graph (or a device flag in eager mode).
+__global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_disp, int in_graph,
+                         int *eager_flags) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Status *st = a.st;
+  int disp = 0, build = 0;
+  if (st->error == 0) {
+    if (st->list_stale) {
+      build = 1;
+    } else {
+      if (st->budget > 0.0) {
+        const double vmax = sqrt(__longlong_as_double((long long)st->vmax2_bits));
+        if (vmax * 2.0 * b.dt > b.buffer_length) {
+          st->too_fast_v = vmax;
+          atomicOr(&st->error, kErrTooFast);
+        } else {
+          st->budget = st->budget - vmax * 2.0 * b.dt;
+        }
+      }
+      if (st->error == 0 && st->budget < 0.0) {
+        disp = 1;
+        st->dr2max_bits = 0ull;
+        st->cand_weighted = 0;
+        st->cand_n = 0;
+        st->disp_checks++;
+      }
+    }
+  }
+  st->want_build = build;
+  st->vmax2_bits = 0ull;
+  if (in_graph) cudaGraphSetConditional(h_disp, disp);
+  else eager_flags[0] = disp;
+}
+
+// Sets the rebuild condition of this step from the expiry and displacement
+// decisions.
+__global__ void k_decide(Arrays a, cudaGraphConditionalHandle h_build, int in_graph, int *eager_flags) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int build = (a.st->error == 0) && a.st->want_build;
+  if (in_graph) cudaGraphSetConditional(h_build, build);
+  else eager_flags[1] = build;
+}
+
+// PairList::CheckByDisplacement, first pass: max |q_old - q|^2 (src/pairlist.cc:67-84).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_disp_max(Arrays a, int n) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  double d2 = 0.0;
+  if (i < n) {
+    const double4 q = a.q[i], o = a.q_old[i];
+    const double dx = dsub(o.x, q.x), dy = dsub(o.y, q.y), dz = dsub(o.z, q.z);
+    d2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+  }
+  block_max_to<BLOCK>(&a.st->dr2max_bits, d2);
+}
+
+// Second pass: atoms that moved more than BufferLength - sqrt(dr2_max)
+// (src/pairlist.cc:86-97).  Each real atom stands for its ghost images too,
+// so it is counted with its image multiplicity, as the reference's loop over
+// real + ghost atoms counts it.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_disp_collect(Arrays a, Box b, int n, int cand_cap) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  bool is_cand = false;
+  int m = 0;
+  if (i < n) {
+    const double dr2_max = __longlong_as_double((long long)a.st->dr2max_bits);
+    const double c = b.buffer_length - sqrt(dr2_max);
+    const double c_d2 = c * c;
+    const double4 q = a.q[i], o = a.q_old[i];
+    const double dx = dsub(o.x, q.x), dy = dsub(o.y, q.y), dz = dsub(o.z, q.z);
+    const double d2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+    is_cand = d2 > c_d2;
+    m = is_cand ? (int)a.mult[i] : 0;
+  }
+  const unsigned ball = __ballot_sync(0xffffffffu, is_cand);
+  const int wsum = __reduce_add_sync(0xffffffffu, m);
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0 && ball) {
+    base = atomicAdd(&a.st->cand_n, __popc(ball));
+    atomicAdd(&a.st->cand_weighted, wsum);
+  }
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (is_cand) {
+    const int k = base + __popc(ball & ((1u << lane) - 1u));
+    if (k < cand_cap) a.cand[k] = i;
+  }
+}
+
+// Third pass, one block: expired if the candidate count reaches
+// min(total atoms incl. images, CheckListLength), or if a candidate pair that
+// was at least SearchLength apart at the last build is now inside the
+// cut-off (src/pairlist.cc:86-121).  Minimum image replaces the ghost copies.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_disp_pairs(Arrays a, Box b) {
+  __shared__ volatile int found;
+  if (threadIdx.x == 0) found = 0;
+  __syncthreads();
+  Status *st = a.st;
+  const long long tn = st->total_images;
+  const int nl = (int)((tn > b.check_list_length) ? b.check_list_length : tn);
+  if (st->cand_weighted >= nl) {
+    if (threadIdx.x == 0) found = 1;
+  } else {
+    const int l = min(st->cand_n, b.check_list_length);
+    const long long npairs = (long long)l * (l - 1) / 2;
+    for (long long p = threadIdx.x; p < npairs && !found; p += BLOCK) {
+      // unrank p -> (r, c) with r < c
+      long long r = (long long)((2.0 * l - 1.0 - sqrt((2.0 * l - 1.0) * (2.0 * l - 1.0) - 8.0 * p)) * 0.5);
+      if (r < 0) r = 0;
+      while (r > 0 && r * (2LL * l - r - 1) / 2 > p) r--;
+      while ((r + 1) * (2LL * l - r - 2) / 2 <= p) r++;
+      const long long c = p - r * (2LL * l - r - 1) / 2 + r + 1;
+      if (r >= l || c >= l || c <= r) continue;
+      const int i1 = a.cand[r], i2 = a.cand[c];
+      const double4 o1 = a.q_old[i1], o2 = a.q_old[i2];
+      double dx = o1.x - image_of(o2.x, o1.x, b.L[0], b.hL[0]);
+      double dy = o1.y - image_of(o2.y, o1.y, b.L[1], b.hL[1]);
+      double dz = o1.z - image_of(o2.z, o1.z, b.L[2], b.hL[2]);
+      double dr2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+      if (dr2 < b.sl2) continue;
+      const double4 n1 = a.q[i1], n2 = a.q[i2];
+      dx = n1.x - image_of(n2.x, n1.x, b.L[0], b.hL[0]);
+      dy = n1.y - image_of(n2.y, n1.y, b.L[1], b.hL[1]);
+      dz = n1.z - image_of(n2.z, n1.z, b.L[2], b.hL[2]);
+      dr2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+      if (dr2 < b.rc2) found = 1;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && found) st->want_build = 1;
+}
+
+// Rebuild 1/6: wrap into [0,L] (Variables::AdjustPeriodicBoundary,
+// src/variables.cc:63-84), validity check, cell index and rank inside the cell.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_cell_assign(Arrays a, Box b, int n) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= n || a.st->error) return;
+  double4 q = a.q[i];
+  double x[3] = {q.x, q.y, q.z};
+  int cc[3];
+  bool bad = false;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    if (!isfinite(x[d])) {
+      atomicOr(&a.st->error, kErrNonFinite);
+      return;
+    }
+    if (x[d] < 0.0) x[d] = dadd(x[d], b.L[d]);
+    else if (x[d] > b.L[d]) x[d] = dsub(x[d], b.L[d]);
+    bad |= (x[d] < 0.0 || x[d] > b.L[d]);
+    cc[d] = cell_coord(x[d], b.inv_cs[d], b.ms[d]);
+  }
+  if (bad) {
+    atomicOr(&a.st->error, kErrInvalidPosition);
+    return;
+  }
+  q.x = x[0]; q.y = x[1]; q.z = x[2];
+  a.q[i] = q;
+  const int c = (cc[2] * b.ms[1] + cc[1]) * b.ms[0] + cc[0];
+  a.cell[i] = c;
+  a.slot[i] = atomicAdd(&a.cell_count[c], 1);
+}
+
+// Rebuild 2/6: exclusive scan of the cell counts, one block.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scan_cells(Arrays a, int ncell) {
+  __shared__ int sums[BLOCK];
+  const int t = threadIdx.x;
+  const int chunk = (ncell + BLOCK - 1) / BLOCK;
+  const int beg = min(t * chunk, ncell), end = min(beg + chunk, ncell);
+  int s = 0;
+  for (int c = beg; c < end; c++) s += a.cell_count[c];
+  sums[t] = s;
+  __syncthreads();
+  for (int off = 1; off < BLOCK; off <<= 1) {
+    int x = (t >= off) ? sums[t - off] : 0;
+    __syncthreads();
+    sums[t] += x;
+    __syncthreads();
+  }
+  int run = sums[t] - s;
+  for (int c = beg; c < end; c++) {
+    a.cell_start[c] = run;
+    run += a.cell_count[c];
+  }
+  if (t == BLOCK - 1) a.cell_start[ncell] = sums[t];
+}
+
+// Rebuild 3/6: scatter old slots to their cell ranges.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scatter(Arrays a, int n) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= n || a.st->error) return;
+  a.perm[a.cell_start[a.cell[i]] + a.slot[i]] = i;
+}
+
+// Rebuild 4/6: order every cell by upload id (one warp per cell), which makes
+// the slot order a function of the state alone, independent of atomics.
+__global__ void k_sort_cells(Arrays a, int ncell) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= ncell || a.st->error) return;
+  const int beg = a.cell_start[warp], cnt = a.cell_start[warp + 1] - beg;
+  for (int base = 0; base < cnt; base += 32) {
+    const int me = base + lane;
+    int my_slot = -1, my_key = 0x7fffffff;
+    if (me < cnt) {
+      my_slot = a.perm[beg + me];
+      my_key = a.ids[my_slot];
+    }
+    int rank = 0;
+    for (int ob = 0; ob < cnt; ob += 32) {
+      const int other = ob + lane;
+      int okey = 0x7fffffff;
+      if (other < cnt) okey = a.ids[a.perm[beg + other]];
+      for (int k = 0; k < 32; k++) {
+        const int kk = __shfl_sync(0xffffffffu, okey, k);
+        if (ob + k < cnt && kk < my_key) rank++;
+      }
+    }
+    if (me < cnt) a.perm2[beg + rank] = my_slot;
+  }
+}
+
+// Image multiplicity of a wrapped position: the number of ghost copies the
+// reference's six sequential border passes make of it, times itself
+// (src/mdmanager.cc:395-401, MDRect::IsInsideEdge src/mdrect.cc:23-47).
+__device__ __forceinline__ int image_multiplicity(const double x[3], const Box &b) {
+  int m = 1;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const int k = 1 + ((x[d] < b.sl && x[d] > 0.0) ? 1 : 0) +
+                  ((x[d] > b.L[d] - b.sl && x[d] < b.L[d]) ? 1 : 0);
+    m *= k;
+  }
+  return m;
+}
+
+// Rebuild 5/6: gather into cell order (temporary arrays), snapshot q_old
+// (PairList::Init), image multiplicity.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_permute(Arrays a, Box b, int n) {
+  const int s = blockIdx.x * BLOCK + threadIdx.x;
+  int m = 0;
+  if (s < n && !a.st->error) {
+    const int o = a.perm2[s];
+    const double4 q = a.q[o];
+    a.q_tmp[s] = q;
+    a.v_tmp[s] = a.v[o];
+    a.ids_tmp[s] = a.ids[o];
+    a.type_tmp[s] = a.type[o];
+    a.cell_tmp[s] = a.cell[o];
+    a.q_old[s] = q;
+    const double x[3] = {q.x, q.y, q.z};
+    m = image_multiplicity(x, b);
+    a.mult[s] = (unsigned char)m;
+  }
+  const int tot = __reduce_add_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0 && tot) atomicAdd((unsigned long long *)&a.st->total_images, (unsigned long long)tot);
+}
+
+// Rebuild 6/6: full Verlet list.  One thread per atom walks the 27 cells
+// around its own (periodic, >= 3 cells per axis so they are distinct) and
+// keeps partner j when r^2 <= SearchLength^2 with r^2 formed exactly as
+// MeshList::SearchMesh does (src/meshlist.cc:276-289): the ghost image
+// q_j + diff first, then dx = x_i - image, then ((dx*dx + dy*dy) + dz*dz),
+// each operation rounded separately.  Row order: cells in (dz,dy,dx) order,
+// slots ascending.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  int cnt = 0;
+  if (i < n && !a.st->error) {
+  const double4 qi = a.q[i];
+  const int c = a.cell_tmp[i];
+  const int cx = c % b.ms[0], cy = (c / b.ms[0]) % b.ms[1], cz = c / (b.ms[0] * b.ms[1]);
+  const int maxnb = a.maxnb, stride = a.stride;
+  for (int dz = -1; dz <= 1; dz++) {
+    int z = cz + dz;
+    double sz = 0.0;
+    if (z < 0) { z += b.ms[2]; sz = -b.L[2]; } else if (z >= b.ms[2]) { z -= b.ms[2]; sz = b.L[2]; }
+    for (int dy = -1; dy <= 1; dy++) {
+      int y = cy + dy;
+      double sy = 0.0;
+      if (y < 0) { y += b.ms[1]; sy = -b.L[1]; } else if (y >= b.ms[1]) { y -= b.ms[1]; sy = b.L[1]; }
+      for (int dx = -1; dx <= 1; dx++) {
+        int x = cx + dx;
+        double sx = 0.0;
+        if (x < 0) { x += b.ms[0]; sx = -b.L[0]; } else if (x >= b.ms[0]) { x -= b.ms[0]; sx = b.L[0]; }
+        const int nc = (z * b.ms[1] + y) * b.ms[0] + x;
+        const int beg = a.cell_start[nc], end = a.cell_start[nc + 1];
+        for (int j = beg; j < end; j++) {
+          if (j == i) continue;
+          const double4 qj = a.q[j];
+          const double gx = dadd(qj.x, sx), gy = dadd(qj.y, sy), gz = dadd(qj.z, sz);
+          const double ex = dsub(qi.x, gx), ey = dsub(qi.y, gy), ez = dsub(qi.z, gz);
+          const double r2 = dadd(dadd(dmul(ex, ex), dmul(ey, ey)), dmul(ez, ez));
+          if (r2 > b.sl2) continue;
+          if (cnt < maxnb) a.nbr[(size_t)cnt * stride + i] = j;
+          cnt++;
+        }
+      }
+    }
+  }
+  a.nnbr[i] = min(cnt, maxnb);
+  if (cnt > maxnb) atomicOr(&a.st->error, kErrCapacity);
+  }
+  const int wmax = __reduce_max_sync(0xffffffffu, cnt);
+  const int wsum = __reduce_add_sync(0xffffffffu, cnt);
+  if ((threadIdx.x & 31) == 0 && wsum) {
+    atomicMax(&a.st->max_row, wmax);
+    atomicAdd((unsigned long long *)&a.st->list_entries, (unsigned long long)wsum);
+  }
+}
+
+// Before a build: clear the build counters.
+__global__ void k_build_begin(Arrays a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  a.st->max_row = 0;
+  a.st->list_entries = 0;
+  a.st->total_images = 0;
+}
+
+// After a build: fresh skin budget (PairList::Init, src/pairlist.cc:10-23),
+// counters, |v|^2 max for the next expiry test is untouched.
+__global__ void k_build_done(Arrays a, Box b) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Status *st = a.st;
+  if (st->error) return;
+  st->budget = b.buffer_length;
+  st->list_stale = 0;
+  st->rebuilds++;
+}
+
+// q += v dt/2 (ForceCalculator::UpdatePositionHalf, src/fcalculator.cc:17-30);
+// FIX also writes the fixed-point copy used by the FP32-mixed force.
+template <int BLOCK, bool FIX>
+__global__ void __launch_bounds__(BLOCK) k_drift(Arrays a, Box b, int n, int track_vmax) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  double v2 = 0.0;
+  if (i < n && !a.st->error) {
+    const double dt2 = b.dt * 0.5;
+    double4 q = a.q[i];
+    const double4 v = a.v[i];
+    q.x = dadd(q.x, dmul(v.x, dt2));
+    q.y = dadd(q.y, dmul(v.y, dt2));
+    q.z = dadd(q.z, dmul(v.z, dt2));
+    a.q[i] = q;
+    if (FIX) a.qfix[i] = make_int4(fixed_coord(q.x, b.L[0]), fixed_coord(q.y, b.L[1]),
+                                   fixed_coord(q.z, b.L[2]), 0);
+    if (track_vmax) {
+      v2 = dadd(dadd(dmul(v.x, v.x), dmul(v.y, v.y)), dmul(v.z, v.z));
+      if (!isfinite(v2) || !isfinite(q.x + q.y + q.z)) atomicOr(&a.st->error, kErrNonFinite);
+    }
+  }
+  if (track_vmax) block_max_to<BLOCK>(&a.st->vmax2_bits, v2);
+}
+
+// Writes the fixed-point copy of q without moving atoms.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_pack_fix(Arrays a, Box b, int n) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= n) return;
+  const double4 q = a.q[i];
+  a.qfix[i] = make_int4(fixed_coord(q.x, b.L[0]), fixed_coord(q.y, b.L[1]), fixed_coord(q.z, b.L[2]), 0);
+}
+
+enum ForceMode { kKick = 0, kForceOut = 1, kKickNoseHoover = 2, kKickLangevin = 3 };
+
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    const uint32_t lo0 = 0xD2511F53u * c[0], hi0 = __umulhi(0xD2511F53u, c[0]);
+    const uint32_t lo1 = 0xCD9E8D57u * c[2], hi1 = __umulhi(0xCD9E8D57u, c[2]);
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+// Three standard normals for (atom id, step) from one Philox4x32-10 block and
+// two Box-Muller pairs; the same stream as the oracle's ljo_langevin_normals.
+__device__ __forceinline__ void langevin_normals(unsigned long long seed, uint32_t id,
+                                                 unsigned long long step, double z[3]) {
+  uint32_t c[4] = {id, (uint32_t)step, (uint32_t)(step >> 32), 0x4C414E47u};
+  philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const double scale = 2.3283064365386963e-10;
+  const double u0 = ((double)c[0] + 0.5) * scale, u1 = ((double)c[1] + 0.5) * scale;
+  const double u2 = ((double)c[2] + 0.5) * scale, u3 = ((double)c[3] + 0.5) * scale;
+  const double twopi = 6.283185307179586;
+  const double r0 = sqrt(-2.0 * log(u0)), r1 = sqrt(-2.0 * log(u2));
+  z[0] = r0 * cos(twopi * u1);
+  z[1] = r0 * sin(twopi * u1);
+  z[2] = r1 * cos(twopi * u3);
+}
+
+struct Thermo {
+  double gamma, noise_sd;      // Langevin friction and noise amplitude sqrt(2 gamma T / dt)
+  unsigned long long seed;     // Langevin key; the counter is the device step count
+};
+
+// Per-atom epilogue shared by both precisions: apply the kick in the mode's
+// form and emit the quantities the next kernels need.
+template <int MODE>
+__device__ __forceinline__ void finish_atom(Arrays &a, const Box &b, const Thermo &th, int i,
+                                            double fx, double fy, double fz, double &v2,
+                                            double &ke) {
+  if (MODE == kForceOut) {
+    a.v_tmp[i] = make_double4(fx, fy, fz, 0.0);
+    return;
+  }
+  double4 v = a.v[i];
+  double exp1 = 1.0;
+  if (MODE == kKickNoseHoover) {
+    exp1 = exp(-(b.dt * 0.5) * a.st->zeta);
+    v.x = dmul(v.x, exp1); v.y = dmul(v.y, exp1); v.z = dmul(v.z, exp1);
+  }
+  v.x = dadd(v.x, fx); v.y = dadd(v.y, fy); v.z = dadd(v.z, fz);
+  if (MODE == kKickNoseHoover) {
+    v.x = dmul(v.x, exp1); v.y = dmul(v.y, exp1); v.z = dmul(v.z, exp1);
+    ke = dadd(dadd(dmul(dmul(0.5, v.x), v.x), dmul(dmul(0.5, v.y), v.y)), dmul(dmul(0.5, v.z), v.z));
+  }
+  if (MODE == kKickLangevin) {
+    // ForceCalculator::Langevin, src/fcalculator.cc:1001-1017
+    double z[3];
+    langevin_normals(th.seed, (uint32_t)a.ids[i], (unsigned long long)a.st->steps, z);
+    const double dt = b.dt;
+    v.x = dadd(v.x, dmul(dadd(dmul(-th.gamma, v.x), dmul(th.noise_sd, z[0])), dt));
+    v.y = dadd(v.y, dmul(dadd(dmul(-th.gamma, v.y), dmul(th.noise_sd, z[1])), dt));
+    v.z = dadd(v.z, dmul(dadd(dmul(-th.gamma, v.z), dmul(th.noise_sd, z[2])), dt));
+    v2 = dadd(dadd(dmul(v.x, v.x), dmul(v.y, v.y)), dmul(v.z, v.z));
+  }
+  a.v[i] = v;
+}
+
+// FP64 force kick, one thread per atom over its full row.  Every pair term is
+// the reference's (ForceCalculator::CalculateForceNext, src/fcalculator.cc:
+// 228-290): dx = image(q_j) - q_i, r2 = (dx*dx + dy*dy) + dz*dz, skipped if
+// r2 > rc^2, r6 = (r2*r2)*r2, df = ((24 r6 - 48) / ((r6*r6)*r2) + 8 C2) * dt,
+// term = df * dx, all separately rounded; only the summation order differs.
+template <int BLOCK, int MODE>
+__global__ void __launch_bounds__(BLOCK) k_force_fp64(Arrays a, Box b, int n, Thermo th) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  double v2 = 0.0, ke = 0.0;
+  if (i < n && !a.st->error) {
+    const double4 qi = a.q[i];
+    const int nn = a.nnbr[i];
+    const double c2x8 = b.c2 * 8.0;
+    const double dt = (MODE == kForceOut) ? 1.0 : b.dt;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    const int *row = a.nbr + i;
+    int j = nn > 0 ? row[0] : 0;
+    for (int k = 0; k < nn; k++) {
+      const int jn = (k + 1 < nn) ? row[(size_t)(k + 1) * a.stride] : 0;
+      const double4 qj = a.q[j];
+      const double dx = dsub(image_of(qj.x, qi.x, b.L[0], b.hL[0]), qi.x);
+      const double dy = dsub(image_of(qj.y, qi.y, b.L[1], b.hL[1]), qi.y);
+      const double dz = dsub(image_of(qj.z, qi.z, b.L[2], b.hL[2]), qi.z);
+      const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+      j = jn;
+      if (r2 > b.rc2) continue;
+      const double r6 = dmul(dmul(r2, r2), r2);
+      const double df = dmul(dadd(ddiv(dsub(dmul(24.0, r6), 48.0), dmul(dmul(r6, r6), r2)), c2x8), dt);
+      fx = dadd(fx, dmul(df, dx));
+      fy = dadd(fy, dmul(df, dy));
+      fz = dadd(fz, dmul(df, dz));
+    }
+    finish_atom<MODE>(a, b, th, i, fx, fy, fz, v2, ke);
+  }
+  if (MODE == kKickLangevin) block_max_to<BLOCK>(&a.st->vmax2_bits, v2);
+  if (MODE == kKickNoseHoover) {
+    double s[1] = {ke};
+    block_sum_to<BLOCK, 1>(s, a.partials);
+  }
+}
+
+// FP32-mixed force kick.  Displacements come from the fixed-point copy: the
+// wrapped int32 difference is the minimum-image displacement, converted to
+// float and scaled by L/2^32.  Pair forces are FP32; every 8 partners the FP32
+// partial is folded into an FP64 per-atom sum; the kick is FP64.
+template <int BLOCK, int MODE>
+__global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Thermo th) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  double v2 = 0.0, ke = 0.0;
+  if (i < n && !a.st->error) {
+    const int4 pi = a.qfix[i];
+    const int nn = a.nnbr[i];
+    const float sx = b.fix_scale[0], sy = b.fix_scale[1], sz = b.fix_scale[2];
+    const float rc2 = b.rc2f, c2x8 = b.c2x8f;
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    const int *row = a.nbr + i;
+    int k = 0;
+    while (k < nn) {
+      const int kend = min(nn, k + 8);
+      float fx = 0.f, fy = 0.f, fz = 0.f;
+      for (; k < kend; k++) {
+        const int j = __ldg(row + (size_t)k * a.stride);
+        const int4 pj = __ldg(a.qfix + j);
+        const float dx = (float)(pj.x - pi.x) * sx;
+        const float dy = (float)(pj.y - pi.y) * sy;
+        const float dz = (float)(pj.z - pi.z) * sz;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float ir2 = __frcp_rn(r2);
+        const float ir6 = ir2 * ir2 * ir2;
+        float df = fmaf(ir2 * ir6, fmaf(-48.f, ir6, 24.f), c2x8);
+        df = (r2 <= rc2) ? df : 0.f;
+        fx = fmaf(df, dx, fx);
+        fy = fmaf(df, dy, fy);
+        fz = fmaf(df, dz, fz);
+      }
+      Fx += (double)fx;
+      Fy += (double)fy;
+      Fz += (double)fz;
+    }
+    const double dt = (MODE == kForceOut) ? 1.0 : b.dt;
+    finish_atom<MODE>(a, b, th, i, Fx * dt, Fy * dt, Fz * dt, v2, ke);
+  }
+  if (MODE == kKickLangevin) block_max_to<BLOCK>(&a.st->vmax2_bits, v2);
+  if (MODE == kKickNoseHoover) {
+    double s[1] = {ke};
+    block_sum_to<BLOCK, 1>(s, a.partials);
+  }
+}
+
+// Kinetic energy partials (KineticEnergyObserver, src/observer.cc:4-15).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_ke_partial(Arrays a, int n) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  double ke = 0.0;
+  if (i < n) {
+    const double4 v = a.v[i];
+    ke = dadd(dadd(dmul(dmul(0.5, v.x), v.x), dmul(dmul(0.5, v.y), v.y)), dmul(dmul(0.5, v.z), v.z));
+  }
+  double s[1] = {ke};
+  block_sum_to<BLOCK, 1>(s, a.partials);
+}
+
+// Sums nblocks partials in a fixed order; Nose-Hoover: T = KE/N/1.5,
+// zeta += (T - T0)/tau^2 * dt/2 (ForceCalculator::HeatbathZeta, src/fcalculator.cc:979-985).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_zeta(Arrays a, Box b, int nblocks, int n, double aimed_t,
+                                                double tau) {
+  __shared__ double sm[BLOCK];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < nblocks; k += BLOCK) s += a.partials[k];
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int off = BLOCK / 2; off > 0; off >>= 1) {
+    if (threadIdx.x < off) sm[threadIdx.x] += sm[threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && !a.st->error) {
+    const double t = sm[0] / (double)n / 1.5;
+    const double t1 = (t - aimed_t) / (tau * tau);
+    a.st->zeta += t1 * (b.dt * 0.5);
+  }
+}
+
+// Observers: KE, PE, virial per atom over the full list, x 1/2 for pair sums
+// (PotentialEnergyObserver / VirialObserver, src/observer.cc:17-79: each
+// pair term formed as the reference forms it).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_observe(Arrays a, Box b, int n) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  double ke = 0.0, pe = 0.0, vir = 0.0;
+  if (i < n) {
+    const double4 v = a.v[i];
+    ke = dadd(dadd(dmul(dmul(0.5, v.x), v.x), dmul(dmul(0.5, v.y), v.y)), dmul(dmul(0.5, v.z), v.z));
+    const double4 qi = a.q[i];
+    const int nn = a.nnbr[i];
+    for (int k = 0; k < nn; k++) {
+      const int j = a.nbr[(size_t)k * a.stride + i];
+      const double4 qj = a.q[j];
+      const double dx = dsub(qi.x, image_of(qj.x, qi.x, b.L[0], b.hL[0]));
+      const double dy = dsub(qi.y, image_of(qj.y, qi.y, b.L[1], b.hL[1]));
+      const double dz = dsub(qi.z, image_of(qj.z, qi.z, b.L[2], b.hL[2]));
+      const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+      if (r2 > b.rc2) continue;
+      const double r4 = dmul(r2, r2), r6 = dmul(r4, r2), r8 = dmul(r6, r2), r10 = dmul(r8, r2),
+                   r12 = dmul(r10, r2);
+      const double e = dmul(4.0, dadd(dadd(dsub(ddiv(1.0, r12), ddiv(1.0, r6)), dmul(b.c2, r2)), b.c0));
+      pe = dadd(pe, e);
+      const double r6v = dmul(dmul(r2, r2), r2);
+      const double w = dmul(dadd(ddiv(dsub(dmul(24.0, r6v), 48.0), dmul(dmul(r6v, r6v), r2)), b.c2 * 8.0), r2);
+      vir = dadd(vir, w);
+    }
+  }
+  double s[3] = {ke, 0.5 * pe, 0.5 * vir};
+  block_sum_to<BLOCK, 3>(s, a.partials);
+}
+
+// Fixed-order final sum of NSUM-wide partials into out[0..NSUM).
+template <int BLOCK, int NSUM>
+__global__ void __launch_bounds__(BLOCK) k_final_sum(const double *partials, int nblocks, double *out) {
+  __shared__ double sm[NSUM][BLOCK];
+  for (int k = 0; k < NSUM; k++) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += BLOCK) s += partials[(size_t)b * NSUM + k];
+    sm[k][threadIdx.x] = s;
+  }
+  __syncthreads();
+  for (int off = BLOCK / 2; off > 0; off >>= 1) {
+    if (threadIdx.x < off)
+      for (int k = 0; k < NSUM; k++) sm[k][threadIdx.x] += sm[k][threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < NSUM; k++) out[k] = sm[k][0];
+}
+
+// End of step bookkeeping (MDManager::Calculate: s_time += TimeStep).
+__global__ void k_step_done(Arrays a, Box b) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (a.st->error) return;
+  a.st->steps++;
+  a.st->sim_time += b.dt;
+}
+
+// HeatbathMomenta alone (src/fcalculator.cc:987-999).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scale_v(Arrays a, int n, double dt2) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= n) return;
+  const double e = exp(-dt2 * a.st->zeta);
+  double4 v = a.v[i];
+  v.x = dmul(v.x, e); v.y = dmul(v.y, e); v.z = dmul(v.z, e);
+  a.v[i] = v;
+}
+
+}  // namespace mdg
