@@ -192,6 +192,10 @@ def main():
     ap.add_argument("--md-steps-per-step", type=int, default=MD_STEPS_PER_STEP)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cells", type=int, default=80, help="FCC cells per axis (80 = 2,048,000 atoms)")
+    ap.add_argument("--precision", choices=["both", "fp32", "fp64"], default="both",
+                    help="restrict the timed runs (profiling); the JSON line needs both")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end run (profiling)")
+    ap.add_argument("--no-force-error", action="store_true", help="skip the FP32-vs-FP64 force check")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     from mdacp_b200 import workloads as W
@@ -281,7 +285,11 @@ def main_mdg(args, ws, rank, local, state, config):
     n = state.n
     sampler = ClockSampler(local)
     result = {}
-    for prec_name, prec in (("fp32", M.FP32_MIXED), ("fp64", M.FP64)):
+    clocks = None
+    runs = [("fp32", M.FP32_MIXED), ("fp64", M.FP64)]
+    if args.precision != "both":
+        runs = [r for r in runs if r[0] == args.precision]
+    for prec_name, prec in runs:
         s = M.System(state.L, cutoff=state.rc, time_step=state.dt, capacity=n, precision=prec, device=local)
         s.set_state(state.q, state.v)
         if prec_name == "fp32":
@@ -294,6 +302,16 @@ def main_mdg(args, ws, rank, local, state, config):
         result[prec_name] = dict(ms=ms_max, value=ws * n * md_steps / (ms_max * 1e-3), force_ms=fms,
                                  force_launches=flaunch, launches=launches, info0=info0, info1=info1)
         s.close()
+
+    if args.precision != "both" or args.no_e2e or args.no_force_error:
+        for name, r in result.items():
+            if rank == 0:
+                print(json.dumps({"profiling_run": name, "ms_per_md_step": r["ms"] / (args.steps * args.md_steps_per_step),
+                                  "value": r["value"], "force_ms_avg": r["force_ms"] / max(1, r["force_launches"]),
+                                  "rebuilds": r["info1"]["rebuilds"] - r["info0"]["rebuilds"]}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
 
     # end to end through the C ABI from pinned host buffers (FP32-mixed path)
     s = M.System(state.L, cutoff=state.rc, time_step=state.dt, capacity=n, precision=M.FP32_MIXED, device=local)
