@@ -116,6 +116,11 @@ mdg_status mdg_heatbath_momenta(mdg_handle *h);
 mdg_status mdg_langevin(mdg_handle *h);
 mdg_status mdg_get_zeta(mdg_handle *h, double *zeta);
 mdg_status mdg_set_zeta(mdg_handle *h, double zeta);
+/* Replaces: MDManager::SetControlTemperature / SetAimedTemperature
+   (include/mdmanager.h:78-79) and the HeatbathType/HeatbathTau/HeatbathGamma
+   fields of SimulationInfo: switches the thermostat of later steps. */
+mdg_status mdg_set_control(mdg_handle *h, int thermostat, double aimed_temperature,
+                           double heatbath_tau, double heatbath_gamma);
 
 /* Replaces: MDManager::Calculate (src/mdmanager.cc:153-186) called nsteps
    times: expiry check, conditional rebuild, half drift, force kick (NVE,
@@ -140,6 +145,13 @@ mdg_status mdg_observe(mdg_handle *h, double *ke, double *pe, double *virial);
    the partner within SearchLength; *count returns the total, at most cap
    entries are written. */
 mdg_status mdg_get_pairs(mdg_handle *h, int *key, int *partner, int64_t cap, int64_t *count);
+
+/* The full Verlet list in the current slot order (the order mdg_get_state
+   returns): row_len[i] partners of slot i, concatenated in `partners`
+   (slot indices).  *count returns the total; at most cap entries are
+   written.  A half list with key < partner is the reference's
+   key_partner_pairs / sorted_list (src/meshlist.cc:67-104, 555-583). */
+mdg_status mdg_get_list(mdg_handle *h, int *row_len, int *partners, int64_t cap, int64_t *count);
 
 typedef struct {
   int n;                  /* atoms */

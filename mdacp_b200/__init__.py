@@ -120,6 +120,8 @@ SIGNATURES = {
     "mdg_langevin": (ctypes.c_int, [_H]),
     "mdg_get_zeta": (ctypes.c_int, [_H, _DP]),
     "mdg_set_zeta": (ctypes.c_int, [_H, ctypes.c_double]),
+    "mdg_set_control": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+    "mdg_get_list": (ctypes.c_int, [_H, _IP, _IP, ctypes.c_int64, _I64P]),
     "mdg_calculate": (ctypes.c_int, [_H, ctypes.c_int]),
     "mdg_forces": (ctypes.c_int, [_H, _DP]),
     "mdg_observe": (ctypes.c_int, [_H, _DP, _DP, _DP]),
@@ -312,6 +314,28 @@ class System:
         p = np.empty(cnt.value, dtype=np.int32)
         self._check(self.lib.mdg_get_pairs(self.h, _i(k), _i(p), cnt.value, ctypes.byref(cnt)))
         return k, p
+
+    def set_control(self, thermostat, aimed_temperature=1.0, heatbath_tau=0.1, heatbath_gamma=0.1):
+        self._check(self.lib.mdg_set_control(self.h, int(thermostat), float(aimed_temperature),
+                                             float(heatbath_tau), float(heatbath_gamma)))
+
+    def langevin(self):
+        self._check(self.lib.mdg_langevin(self.h))
+
+    def heatbath_momenta(self):
+        self._check(self.lib.mdg_heatbath_momenta(self.h))
+
+    def heatbath_zeta(self, temperature):
+        self._check(self.lib.mdg_heatbath_zeta(self.h, float(temperature)))
+
+    def neighbor_list(self):
+        """Full list in slot order: (row lengths, concatenated partner slots)."""
+        cnt = ctypes.c_int64()
+        self._check(self.lib.mdg_get_list(self.h, None, None, 0, ctypes.byref(cnt)))
+        rows = np.empty(self.n, dtype=np.int32)
+        part = np.empty(cnt.value, dtype=np.int32)
+        self._check(self.lib.mdg_get_list(self.h, _i(rows), _i(part), cnt.value, ctypes.byref(cnt)))
+        return rows, part
 
     def zeta(self) -> float:
         z = ctypes.c_double()

@@ -701,10 +701,54 @@ mdg_status mdg_heatbath_momenta(mdg_handle *h) {
 }
 
 mdg_status mdg_langevin(mdg_handle *h) {
-  // The Langevin update is fused into the force kick of mdg_calculate; alone
-  // it needs a kick of zero force, which is what a force-free step is not:
-  // expose it only through the full step.
-  return fail(h, MDG_ERR_STATE, "mdg_langevin: use mdg_calculate with thermostat MDG_LANGEVIN");
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (h->n == 0) return MDG_OK;
+  k_langevin<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n, thermo_of(h));
+  CUDA_TRY(h, cudaGetLastError());
+  return MDG_OK;
+}
+
+mdg_status mdg_set_control(mdg_handle *h, int thermostat, double aimed_temperature, double heatbath_tau,
+                           double heatbath_gamma) {
+  if (!h || thermostat < MDG_NVE || thermostat > MDG_LANGEVIN) return MDG_ERR_INVALID_ARGUMENT;
+  if (thermostat != h->prm.thermostat || aimed_temperature != h->prm.aimed_temperature ||
+      heatbath_tau != h->prm.heatbath_tau || heatbath_gamma != h->prm.heatbath_gamma) {
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->prm.thermostat = thermostat;
+    h->prm.aimed_temperature = aimed_temperature;
+    h->prm.heatbath_tau = heatbath_tau;
+    h->prm.heatbath_gamma = heatbath_gamma;
+    destroy_graph(h);
+  }
+  return MDG_OK;
+}
+
+mdg_status mdg_get_list(mdg_handle *h, int *row_len, int *partners, int64_t cap, int64_t *count) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (!count || cap < 0) return MDG_ERR_INVALID_ARGUMENT;
+  *count = 0;
+  if (h->n == 0) return MDG_OK;
+  if ((r = ensure_list(h))) return r;
+  const int n = h->n, stride = h->a.stride;
+  std::vector<int> nn(n);
+  CUDA_TRY(h, cudaMemcpyAsync(nn.data(), h->a.nnbr, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  const int maxrow = *std::max_element(nn.begin(), nn.end());
+  std::vector<int> tab((size_t)maxrow * stride);
+  if (maxrow > 0)
+    CUDA_TRY(h, cudaMemcpy(tab.data(), h->a.nbr, sizeof(int) * (size_t)maxrow * stride, cudaMemcpyDeviceToHost));
+  int64_t c = 0;
+  for (int i = 0; i < n; i++) {
+    if (row_len) row_len[i] = nn[i];
+    for (int k = 0; k < nn[i]; k++) {
+      if (c < cap && partners) partners[c] = tab[(size_t)k * stride + i];
+      c++;
+    }
+  }
+  *count = c;
+  return MDG_OK;
 }
 
 mdg_status mdg_get_zeta(mdg_handle *h, double *zeta) {

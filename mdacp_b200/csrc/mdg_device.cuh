@@ -807,6 +807,23 @@ __global__ void k_step_done(Arrays a, Box b) {
   a.st->sim_time += b.dt;
 }
 
+// Langevin alone (ForceCalculator::Langevin, src/fcalculator.cc:1001-1017),
+// for callers that run the step piece by piece; the noise counter is the
+// device step count, as in the fused kick.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_langevin(Arrays a, Box b, int n, Thermo th) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= n || a.st->error) return;
+  double4 v = a.v[i];
+  double z[3];
+  langevin_normals(th.seed, (uint32_t)a.ids[i], (unsigned long long)a.st->steps, z);
+  const double dt = b.dt;
+  v.x = dadd(v.x, dmul(dadd(dmul(-th.gamma, v.x), dmul(th.noise_sd, z[0])), dt));
+  v.y = dadd(v.y, dmul(dadd(dmul(-th.gamma, v.y), dmul(th.noise_sd, z[1])), dt));
+  v.z = dadd(v.z, dmul(dadd(dmul(-th.gamma, v.z), dmul(th.noise_sd, z[2])), dt));
+  a.v[i] = v;
+}
+
 // HeatbathMomenta alone (src/fcalculator.cc:987-999).
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_scale_v(Arrays a, int n, double dt2) {

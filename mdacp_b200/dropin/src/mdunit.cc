@@ -1,0 +1,141 @@
+// Drop-in MDUnit (interface of include/mdunit.h:16-104 in the reference):
+// one unit spanning the whole periodic box, backed by one GPU handle.
+#include "mdunit.h"
+
+#include <cstdio>
+#include <cstring>
+
+#include "mpistream.h"
+
+MDUnit::MDUnit(int id_, SimulationInfo *si, ParaInfo *pi, int capacity, int precision_)
+    : sinfo(si), pinfo(pi), id(id_), dev(nullptr), precision(precision_) {
+  vars = new Variables(capacity);
+  plist = new PairList();
+  int grid_size[D], grid_position[D];
+  pinfo->GetGridSize(grid_size);
+  pinfo->GetGridPosition(id, grid_position);
+  double s[D], e[D];
+  for (int d = 0; d < D; d++) {
+    const double ul = sinfo->L[d] / static_cast<double>(grid_size[d]);
+    s[d] = ul * static_cast<double>(grid_position[d]);
+    e[d] = s[d] + ul;
+  }
+  myrect = MDRect(s, e);
+  mesh = new MeshList(sinfo, myrect);
+  CreateDevice();
+}
+
+MDUnit::~MDUnit(void) {
+  if (dev) {
+    vars->SyncToDevice();  // run queued steps before the state goes away
+    mdg_destroy(dev);
+  }
+  delete vars;
+  delete mesh;
+  delete plist;
+}
+
+int thermostat_of(SimulationInfo *sinfo) {
+  if (!sinfo->ControlTemperature) return MDG_NVE;
+  return sinfo->HeatbathType == HT_LANGEVIN ? MDG_LANGEVIN : MDG_NOSE_HOOVER;
+}
+
+void MDUnit::CreateDevice(void) {
+  mdg_params prm;
+  mdg_default_params(&prm);
+  prm.capacity = vars->GetCapacity();
+  for (int d = 0; d < 3; d++) prm.L[d] = sinfo->L[d];
+  prm.cutoff = CUTOFF_LENGTH;
+  prm.buffer_length = sinfo->BufferLength;
+  prm.time_step = sinfo->TimeStep;
+  prm.precision = precision;
+  prm.thermostat = thermostat_of(sinfo);
+  prm.aimed_temperature = sinfo->AimedTemperature;
+  prm.heatbath_tau = sinfo->HeatbathTau;
+  prm.heatbath_gamma = sinfo->HeatbathGamma;
+  prm.check_list_length = sinfo->CheckListLength;
+  prm.seed = static_cast<uint64_t>(id);
+  mdg_handle *h = nullptr;
+  mdg_check(nullptr, mdg_create(&prm, &h), "mdg_create");
+  dev = h;
+  vars->AttachDevice(dev);
+  mesh->Attach(vars);
+}
+
+void MDUnit::SetControl(void) {
+  mdg_check(dev, mdg_set_control(dev, thermostat_of(sinfo), sinfo->AimedTemperature, sinfo->HeatbathTau,
+                                 sinfo->HeatbathGamma), "mdg_set_control");
+}
+
+Variables *MDUnit::GetVariables(void) {
+  // the caller may read and write the arrays: hand over a current mirror and
+  // upload it again before the next device step
+  vars->SyncToHost();
+  vars->MarkHostDirty();
+  return vars;
+}
+
+void MDUnit::AddParticle(double x[D], int type) {
+  double v[D] = {0.0, 0.0, 0.0, 0.0};
+  AddParticle(x, v, type);
+}
+
+void MDUnit::AddParticle(double x[D], double v[D], int type) {
+  if (myrect.IsInside(x)) {
+    vars->SyncToHost();
+    vars->AddParticle(x, v, type);
+  }
+}
+
+void MDUnit::SaveAsCdview(std::ofstream &ofs) {
+  vars->SyncToHost();
+  double(*q)[D] = vars->q;
+  double(*p)[D] = vars->p;
+  const int pn = vars->GetParticleNumber();
+  for (int i = 0; i < pn; i++) {
+    ofs << "0 " << vars->type[i] << " " << q[i][X] << " " << q[i][Y] << " " << q[i][Z] << " " << p[i][X]
+        << " " << p[i][Y] << " " << p[i][Z] << "\n";
+  }
+}
+
+void MDUnit::SaveConfiguration(void) {
+  vars->SyncToHost();
+  char filename[256];
+  snprintf(filename, sizeof filename, "conf%03d.cnf", id);
+  std::ofstream fs(filename);
+  vars->SaveConfiguration(fs);
+}
+
+double MDUnit::ObserveDouble(DoubleObserver *obs) {
+  if (obs->OnDevice()) {
+    vars->SyncToDevice();
+  } else {
+    vars->SyncToHost();
+  }
+  return obs->Observe(vars, mesh);
+}
+
+void MDUnit::Execute(Executor *ex) {
+  vars->SyncToHost();
+  ex->Execute(this);
+  vars->MarkHostDirty();
+}
+
+void MDUnit::MakePairList(void) {
+  plist->Init(vars, sinfo);
+  mesh->MakeList(vars, sinfo, myrect);
+}
+
+void MDUnit::ChangeScale(double alpha) {
+  vars->SyncToHost();
+  myrect.ChangeScale(alpha);
+  vars->ChangeScale(alpha);
+  mesh->ChangeScale(sinfo, myrect);
+  // the box is part of the device handle: rebuild it with the new lengths
+  const double zeta = vars->Zeta;
+  mdg_destroy(dev);
+  dev = nullptr;
+  CreateDevice();
+  vars->Zeta = zeta;
+  vars->MarkHostDirty();
+}

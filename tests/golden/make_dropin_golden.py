@@ -1,0 +1,53 @@
+"""Runs the reference MDACP (CPU, plain build compiled from its sources into
+oracle/_ref/) on the project inputs that tests/test_dropin.py feeds to the
+GPU drop-in binary, and stores the reference's stdout as fixtures.  Both
+sides start from the same state: the projects build it with the
+reference's own seeded generators (one unit, id 0).
+
+Usage:  python tests/golden/make_dropin_golden.py   (needs oracle/_ref built)
+"""
+from __future__ import annotations
+
+import os
+import pathlib
+import subprocess
+import sys
+import tempfile
+
+ROOT = pathlib.Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+OUT = pathlib.Path(__file__).resolve().parent
+
+# name -> (cut-off, input lines)
+CASES = {
+    "benchmark_rc25": (2.5, {"Mode": "Benchmark", "Density": "0.5", "SystemSize": "12",
+                             "TimeStep": "0.005", "ThermalizeLoop": "50", "TotalLoop": "300",
+                             "ObserveLoop": "50", "InitialVelocity": "1.0"}),
+    "langevin_nosehoover_rc25": (2.5, {"Mode": "Langevin", "Density": "0.7", "SystemSize": "12",
+                                       "TimeStep": "0.005", "TotalLoop": "300", "ObserveLoop": "50",
+                                       "InitialVelocity": "1.0", "HeatbathType": "NoseHoover",
+                                       "AimedTemperature": "1.5", "HeatbathTau": "0.1"}),
+    "collision_rc30": (3.0, {"Mode": "Collision", "SystemSize": "40", "TimeStep": "0.005",
+                             "TotalLoop": "300", "ObserveLoop": "50"}),
+}
+
+
+def cfg_text(lines):
+    return "".join(f"{k}={v}\n" for k, v in lines.items())
+
+
+def main():
+    for name, (rc, lines) in CASES.items():
+        tag = {2.5: "25", 3.0: "30"}[rc]
+        binary = ROOT / "oracle" / "_ref" / f"mdacp_rc{tag}_plain"
+        with tempfile.TemporaryDirectory() as wd:
+            (pathlib.Path(wd) / "input.cfg").write_text(cfg_text(lines))
+            out = subprocess.run([str(binary), "-i", "input.cfg"], cwd=wd, capture_output=True, text=True,
+                                 env=dict(os.environ, OMP_NUM_THREADS="1"), check=True)
+        (OUT / f"dropin_{name}.cfg").write_text(cfg_text(lines))
+        (OUT / f"dropin_{name}.ref.txt").write_text(out.stdout)
+        print(name, len(out.stdout.splitlines()), "lines")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,64 @@
+"""The reference's own projects (Benchmark, Langevin with a Nose-Hoover
+bath, Collision) run unchanged on the GPU drop-in (MDManager / MDUnit /
+Variables / MeshList / PairList / ForceCalculator over libmdacp_b200.so) and
+print the same observables as the reference's CPU build on the same input
+(fixtures from tests/golden/make_dropin_golden.py).  The reference prints 6
+significant digits, so the comparison is at that precision."""
+from __future__ import annotations
+
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+GOLDEN = ROOT / "tests" / "golden"
+BUILD = ROOT / "mdacp_b200" / "dropin" / "_build"
+CASES = {"benchmark_rc25": "25", "langevin_nosehoover_rc25": "25", "collision_rc30": "30"}
+
+
+def observe_rows(text):
+    rows = []
+    for line in text.splitlines():
+        if "observe" in line and not line.startswith("#"):
+            rows.append([float(x) for x in line.split("#")[0].split()])
+    return np.array(rows)
+
+
+def run_dropin(name, tmp_path, extra=""):
+    binary = BUILD / f"mdacp_rc{CASES[name]}"
+    if not binary.exists():
+        pytest.skip(f"{binary} not built (mdacp_b200/dropin/build_dropin.sh needs the reference tree)")
+    cfg = (GOLDEN / f"dropin_{name}.cfg").read_text() + extra
+    (tmp_path / "input.cfg").write_text(cfg)
+    out = subprocess.run([str(binary), "-i", "input.cfg"], cwd=tmp_path, capture_output=True, text=True,
+                         timeout=600, env=dict(os.environ, OMP_NUM_THREADS="1"))
+    assert out.returncode == 0, out.stdout + out.stderr
+    return out.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_project_runs_unchanged(name, tmp_path):
+    got = observe_rows(run_dropin(name, tmp_path))
+    ref = observe_rows((GOLDEN / f"dropin_{name}.ref.txt").read_text())
+    assert got.shape == ref.shape and got.shape[0] >= 5
+    assert np.allclose(got, ref, rtol=2e-5, atol=2e-5), np.abs(got - ref).max()
+
+
+@pytest.mark.gpu
+def test_benchmark_fp32_mixed_energy(tmp_path):
+    out = run_dropin("benchmark_rc25", tmp_path, extra="Precision=FP32Mixed\n")
+    got = observe_rows(out)
+    ref = observe_rows((GOLDEN / "dropin_benchmark_rc25.ref.txt").read_text())
+    # total energy per atom agrees with the FP64 reference to the FP32 force error
+    assert np.allclose(got[:, 3], ref[:, 3], rtol=1e-4, atol=1e-4)
+    assert "[MUPS]" in out
+
+
+def test_dropin_fixtures_present():
+    for name in CASES:
+        assert (GOLDEN / f"dropin_{name}.cfg").exists()
+        assert observe_rows((GOLDEN / f"dropin_{name}.ref.txt").read_text()).shape[0] >= 5
