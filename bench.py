@@ -196,6 +196,8 @@ def main():
                     help="restrict the timed runs (profiling); the JSON line needs both")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end run (profiling)")
     ap.add_argument("--no-force-error", action="store_true", help="skip the FP32-vs-FP64 force check")
+    ap.add_argument("--eager", action="store_true",
+                    help="launch every kernel from the host instead of CUDA graphs (for profilers)")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     from mdacp_b200 import workloads as W
@@ -292,6 +294,8 @@ def main_mdg(args, ws, rank, local, state, config):
     for prec_name, prec in runs:
         s = M.System(state.L, cutoff=state.rc, time_step=state.dt, capacity=n, precision=prec, device=local)
         s.set_state(state.q, state.v)
+        if args.eager:
+            s.set_graph_mode(False)
         if prec_name == "fp32":
             sampler.start()
         ms, fms, flaunch, launches, info0, info1 = timed_run(s, args, dist, device, torch)

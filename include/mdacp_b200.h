@@ -172,6 +172,12 @@ mdg_status mdg_get_info(mdg_handle *h, mdg_info *info);
    every force kernel when timing is on; mdg_kernel_time returns the summed
    milliseconds and launch count of the force kernel since the last reset. */
 void *mdg_stream(mdg_handle *h);
+/* use_graphs = 1 (default): mdg_calculate runs batches of steps as CUDA
+   graphs with conditional rebuild nodes.  0: every kernel is launched
+   directly from the host, with the skin decision read back each step --
+   the same kernels and results, for profilers that cannot look inside
+   graphs holding conditional nodes. */
+mdg_status mdg_set_graph_mode(mdg_handle *h, int use_graphs);
 mdg_status mdg_set_kernel_timing(mdg_handle *h, int on);
 mdg_status mdg_kernel_time(mdg_handle *h, double *force_ms, int64_t *force_launches,
                            int64_t *kernel_launches);

@@ -128,6 +128,7 @@ SIGNATURES = {
     "mdg_get_pairs": (ctypes.c_int, [_H, _IP, _IP, ctypes.c_int64, _I64P]),
     "mdg_get_info": (ctypes.c_int, [_H, ctypes.POINTER(Info)]),
     "mdg_stream": (ctypes.c_void_p, [_H]),
+    "mdg_set_graph_mode": (ctypes.c_int, [_H, ctypes.c_int]),
     "mdg_set_kernel_timing": (ctypes.c_int, [_H, ctypes.c_int]),
     "mdg_kernel_time": (ctypes.c_int, [_H, _DP, _I64P, _I64P]),
     "mdg_last_error": (ctypes.c_char_p, [_H]),
@@ -349,6 +350,9 @@ class System:
 
     def stream(self):
         return self.lib.mdg_stream(self.h)
+
+    def set_graph_mode(self, use_graphs: bool):
+        self._check(self.lib.mdg_set_graph_mode(self.h, int(bool(use_graphs))))
 
     def set_kernel_timing(self, on: bool):
         self._check(self.lib.mdg_set_kernel_timing(self.h, int(bool(on))))

@@ -43,6 +43,7 @@ struct mdg_handle {
   cudaGraphExec_t exec = nullptr;
   bool graph_dirty = true;
   bool timing = false;
+  bool use_graphs = true;
   std::vector<cudaEvent_t> ev;        // force-kernel start/stop per step of the graph
   double force_ms = 0.0;
   int64_t force_launches = 0;
@@ -178,14 +179,21 @@ void launch_build(mdg_handle *h, cudaStream_t s) {
   k_build_done<<<1, 32, 0, s>>>(a, h->box);
 }
 
+// drift: also apply the second half drift in the same pass (FP32-mixed only;
+// returns false when the caller still has to launch the drift).
 template <int MODE>
-void launch_force_mode(mdg_handle *h, cudaStream_t s, const Thermo &th) {
+bool launch_force_mode(mdg_handle *h, cudaStream_t s, const Thermo &th, bool drift = false) {
   const int n = h->n;
   const int nb = blocks_for(n, kForceBlock);
-  if (h->prm.precision == MDG_FP32_MIXED)
-    k_force_fp32<kForceBlock, MODE><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th);
-  else
-    k_force_fp64<kForceBlock, MODE><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th);
+  if (h->prm.precision == MDG_FP32_MIXED) {
+    if (drift)
+      k_force_fp32<kForceBlock, MODE, true><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th);
+    else
+      k_force_fp32<kForceBlock, MODE, false><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th);
+    return drift;
+  }
+  k_force_fp64<kForceBlock, MODE><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th);
+  return false;
 }
 
 Thermo thermo_of(const mdg_handle *h) {
@@ -224,12 +232,16 @@ int launch_step_tail(mdg_handle *h, cudaStream_t s, cudaEvent_t ev_start, cudaEv
     k_ke_partial<kBlock><<<nbk, kBlock, 0, s>>>(h->a, n);
     k_zeta<1024><<<1, 1024, 0, s>>>(h->a, h->box, nbk, n, h->prm.aimed_temperature, h->prm.heatbath_tau);
     rec(ev_start);
-    launch_force_mode<kKickNoseHoover>(h, s, th);
+    // the second drift does not read zeta, so it may precede the zeta update
+    const bool drifted = launch_force_mode<kKickNoseHoover>(h, s, th, true);
     rec(ev_stop);
     k_zeta<1024><<<1, 1024, 0, s>>>(h->a, h->box, blocks_for(n, kForceBlock), n,
                                      h->prm.aimed_temperature, h->prm.heatbath_tau);
-    launch_drift(h, s, false, 1);
-    launches += 5;
+    launches += 4;
+    if (!drifted) {
+      launch_drift(h, s, false, 1);
+      launches++;
+    }
   } else if (h->prm.thermostat == MDG_LANGEVIN) {
     rec(ev_start);
     launch_force_mode<kKickLangevin>(h, s, th);
@@ -237,10 +249,13 @@ int launch_step_tail(mdg_handle *h, cudaStream_t s, cudaEvent_t ev_start, cudaEv
     launches += 1;
   } else {
     rec(ev_start);
-    launch_force_mode<kKick>(h, s, th);
+    const bool drifted = launch_force_mode<kKick>(h, s, th, true);
     rec(ev_stop);
-    launch_drift(h, s, false, 1);
-    launches += 2;
+    launches += 1;
+    if (!drifted) {
+      launch_drift(h, s, false, 1);
+      launches++;
+    }
   }
   k_step_done<<<1, 32, 0, s>>>(h->a, h->box);
   return launches + 1;
@@ -780,10 +795,10 @@ mdg_status mdg_calculate(mdg_handle *h, int nsteps) {
   for (int attempt = 0; attempt < 8; attempt++) {
     long long left = target - st.steps;
     if (left <= 0) break;
-    if (left >= kStepsPerGraph && h->graph_dirty) {
+    if (h->use_graphs && left >= kStepsPerGraph && h->graph_dirty) {
       if ((r = build_graph(h))) return r;
     }
-    while (left >= kStepsPerGraph) {
+    while (h->use_graphs && left >= kStepsPerGraph) {
       CUDA_TRY(h, cudaGraphLaunch(h->exec, h->stream));
       h->kernel_launches += h->graph_kernel_count;
       left -= kStepsPerGraph;
@@ -899,6 +914,12 @@ mdg_status mdg_get_info(mdg_handle *h, mdg_info *info) {
 }
 
 void *mdg_stream(mdg_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+mdg_status mdg_set_graph_mode(mdg_handle *h, int use_graphs) {
+  if (!h) return MDG_ERR_INVALID_ARGUMENT;
+  h->use_graphs = use_graphs != 0;
+  return MDG_OK;
+}
 
 mdg_status mdg_set_kernel_timing(mdg_handle *h, int on) {
   if (!h) return MDG_ERR_INVALID_ARGUMENT;

@@ -665,11 +665,32 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp64(Arrays a, Box b, int n, Th
   }
 }
 
-// FP32-mixed force kick.  Displacements come from the fixed-point copy: the
-// wrapped int32 difference is the minimum-image displacement, converted to
-// float and scaled by L/2^32.  Pair forces are FP32; every 8 partners the FP32
-// partial is folded into an FP64 per-atom sum; the kick is FP64.
-template <int BLOCK, int MODE>
+// One FP32 pair term from fixed-point positions: the wrapped int32
+// difference is the minimum-image displacement in units of L/2^32.
+// `valid` masks padding lanes of the unrolled loop.
+__device__ __forceinline__ void lj_pair_fp32(const int4 &pi, const int4 &pj, bool valid, float sx, float sy,
+                                             float sz, float rc2, float c2x8, float &fx, float &fy, float &fz) {
+  const float dx = (float)(pj.x - pi.x) * sx;
+  const float dy = (float)(pj.y - pi.y) * sy;
+  const float dz = (float)(pj.z - pi.z) * sz;
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float ir2 = __frcp_rn(r2);
+  const float ir6 = ir2 * ir2 * ir2;
+  float df = fmaf(ir2 * ir6, fmaf(-48.f, ir6, 24.f), c2x8);
+  df = (valid && r2 <= rc2) ? df : 0.f;
+  fx = fmaf(df, dx, fx);
+  fy = fmaf(df, dy, fy);
+  fz = fmaf(df, dz, fz);
+}
+
+// FP32-mixed force kick.  Displacements come from the fixed-point copy (no
+// ghost atoms, no shift codes).  The row is walked four partners at a time
+// with the next four indices loaded ahead; FP32 partial sums over 8 partners
+// are folded into an FP64 per-atom sum; the kick is FP64.  With DRIFT the
+// second half drift q += v dt/2 and the |v| maximum of the step are done in
+// the same pass: this kernel reads only the fixed-point copy, so moving q
+// here races with no other thread.
+template <int BLOCK, int MODE, bool DRIFT>
 __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Thermo th) {
   const int i = blockIdx.x * BLOCK + threadIdx.x;
   double v2 = 0.0, ke = 0.0;
@@ -678,35 +699,53 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Th
     const int nn = a.nnbr[i];
     const float sx = b.fix_scale[0], sy = b.fix_scale[1], sz = b.fix_scale[2];
     const float rc2 = b.rc2f, c2x8 = b.c2x8f;
-    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
     const int *row = a.nbr + i;
-    int k = 0;
-    while (k < nn) {
-      const int kend = min(nn, k + 8);
-      float fx = 0.f, fy = 0.f, fz = 0.f;
-      for (; k < kend; k++) {
-        const int j = __ldg(row + (size_t)k * a.stride);
-        const int4 pj = __ldg(a.qfix + j);
-        const float dx = (float)(pj.x - pi.x) * sx;
-        const float dy = (float)(pj.y - pi.y) * sy;
-        const float dz = (float)(pj.z - pi.z) * sz;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const float ir2 = __frcp_rn(r2);
-        const float ir6 = ir2 * ir2 * ir2;
-        float df = fmaf(ir2 * ir6, fmaf(-48.f, ir6, 24.f), c2x8);
-        df = (r2 <= rc2) ? df : 0.f;
-        fx = fmaf(df, dx, fx);
-        fy = fmaf(df, dy, fy);
-        fz = fmaf(df, dz, fz);
+    const size_t st = (size_t)a.stride;
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+    int n0 = (0 < nn) ? __ldg(row) : i;
+    int n1 = (1 < nn) ? __ldg(row + st) : i;
+    int n2 = (2 < nn) ? __ldg(row + 2 * st) : i;
+    int n3 = (3 < nn) ? __ldg(row + 3 * st) : i;
+    for (int k = 0; k < nn; k += 4) {
+      const int j0 = n0, j1 = n1, j2 = n2, j3 = n3;
+      n0 = (k + 4 < nn) ? __ldg(row + (size_t)(k + 4) * st) : i;
+      n1 = (k + 5 < nn) ? __ldg(row + (size_t)(k + 5) * st) : i;
+      n2 = (k + 6 < nn) ? __ldg(row + (size_t)(k + 6) * st) : i;
+      n3 = (k + 7 < nn) ? __ldg(row + (size_t)(k + 7) * st) : i;
+      const int4 p0 = __ldg(a.qfix + j0);
+      const int4 p1 = __ldg(a.qfix + j1);
+      const int4 p2 = __ldg(a.qfix + j2);
+      const int4 p3 = __ldg(a.qfix + j3);
+      lj_pair_fp32(pi, p0, true, sx, sy, sz, rc2, c2x8, fx, fy, fz);
+      lj_pair_fp32(pi, p1, k + 1 < nn, sx, sy, sz, rc2, c2x8, fx, fy, fz);
+      lj_pair_fp32(pi, p2, k + 2 < nn, sx, sy, sz, rc2, c2x8, fx, fy, fz);
+      lj_pair_fp32(pi, p3, k + 3 < nn, sx, sy, sz, rc2, c2x8, fx, fy, fz);
+      if (k & 4) {
+        Fx += (double)fx;
+        Fy += (double)fy;
+        Fz += (double)fz;
+        fx = fy = fz = 0.f;
       }
-      Fx += (double)fx;
-      Fy += (double)fy;
-      Fz += (double)fz;
     }
+    Fx += (double)fx;
+    Fy += (double)fy;
+    Fz += (double)fz;
     const double dt = (MODE == kForceOut) ? 1.0 : b.dt;
     finish_atom<MODE>(a, b, th, i, Fx * dt, Fy * dt, Fz * dt, v2, ke);
+    if (DRIFT) {
+      const double4 v = a.v[i];
+      double4 q = a.q[i];
+      const double dt2 = b.dt * 0.5;
+      q.x = dadd(q.x, dmul(v.x, dt2));
+      q.y = dadd(q.y, dmul(v.y, dt2));
+      q.z = dadd(q.z, dmul(v.z, dt2));
+      a.q[i] = q;
+      v2 = dadd(dadd(dmul(v.x, v.x), dmul(v.y, v.y)), dmul(v.z, v.z));
+      if (!isfinite(v2) || !isfinite(q.x + q.y + q.z)) atomicOr(&a.st->error, kErrNonFinite);
+    }
   }
-  if (MODE == kKickLangevin) block_max_to<BLOCK>(&a.st->vmax2_bits, v2);
+  if (MODE == kKickLangevin || DRIFT) block_max_to<BLOCK>(&a.st->vmax2_bits, v2);
   if (MODE == kKickNoseHoover) {
     double s[1] = {ke};
     block_sum_to<BLOCK, 1>(s, a.partials);
