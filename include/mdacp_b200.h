@@ -182,6 +182,22 @@ mdg_status mdg_set_kernel_timing(mdg_handle *h, int on);
 mdg_status mdg_kernel_time(mdg_handle *h, double *force_ms, int64_t *force_launches,
                            int64_t *kernel_launches);
 
+/* No counterpart in the reference.  mdg_observe for callers that cannot
+   allocate device memory (they own all of it, or must avoid the implicit
+   synchronisation of cudaMalloc/cudaFree): no handle, all arrays are the
+   caller's DEVICE pointers -- q4, v4 (n x 4 doubles), a CSR full list
+   row_start (n + 1 ints) / partners (row_start[n] ints, indices into q4),
+   out (3 doubles: KE, PE, virial as mdg_observe returns them).  L and cutoff
+   are host values.  Work is queued on `stream` (cudaStream_t, NULL = legacy
+   default stream); out is ready when the stream is.  Scratch is a static
+   device array of 196,608 bytes held by every GPU that loads the library, so
+   n is limited to 2,097,152 (MDG_ERR_CAPACITY above).  The first call on a
+   device sets up the array's address: make it before any stream capture.
+   Calls that overlap on the GPU race on the shared scratch. */
+mdg_status mdg_observe_static(const double *q4, const double *v4, int n, const int *row_start,
+                              const int *partners, const double L[3], double cutoff, double *out,
+                              void *stream);
+
 const char *mdg_last_error(mdg_handle *h);
 const char *mdg_status_string(mdg_status s);
 /* Library version string. */

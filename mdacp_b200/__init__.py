@@ -131,6 +131,8 @@ SIGNATURES = {
     "mdg_set_graph_mode": (ctypes.c_int, [_H, ctypes.c_int]),
     "mdg_set_kernel_timing": (ctypes.c_int, [_H, ctypes.c_int]),
     "mdg_kernel_time": (ctypes.c_int, [_H, _DP, _I64P, _I64P]),
+    "mdg_observe_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_void_p, _DP, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]),
     "mdg_last_error": (ctypes.c_char_p, [_H]),
     "mdg_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "mdg_version": (ctypes.c_char_p, []),
