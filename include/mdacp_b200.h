@@ -46,6 +46,7 @@ enum {
 };
 
 enum { MDG_FP64 = 0, MDG_FP32_MIXED = 1 };
+enum { MDG_OBSERVE_CURRENT = 0, MDG_OBSERVE_GHOST_LAG = 1 };
 enum { MDG_NVE = 0, MDG_NOSE_HOOVER = 1, MDG_LANGEVIN = 2 };
 
 /* Run parameters; the reference's SimulationInfo public fields
@@ -138,6 +139,16 @@ mdg_status mdg_forces(mdg_handle *h, double *f4);
    does (src/mdmanager.cc:520-528): ke = sum 1/2 p^2, pe = sum of pair
    energies, virial = sum(...)/3.  FP64 device reductions. */
 mdg_status mdg_observe(mdg_handle *h, double *ke, double *pe, double *virial);
+
+/* Which positions mdg_observe pairs an atom with across the periodic
+   boundary.  MDG_OBSERVE_CURRENT (default): every atom at its current
+   position.  MDG_OBSERVE_GHOST_LAG: what the reference's observers see after
+   MDManager::Calculate in the NVE and Nose-Hoover branches -- its ghost
+   copies were refreshed after the first half drift (src/mdmanager.cc:165-167),
+   so a partner reached through the boundary sits half a step back,
+   q - v dt/2.  The drop-in classes use GHOST_LAG so that projects print what
+   the reference prints. */
+mdg_status mdg_set_observer_mode(mdg_handle *h, int mode);
 
 /* Pairlist readout for parity (MeshList::GetPairNumber, GetKeyPointer,
    GetPartnerNumber, GetSortedList, include/meshlist.h:70-91).  Directed

@@ -30,6 +30,7 @@ __all__ = [
 LIB_PATH = pathlib.Path(__file__).resolve().parent / "libmdacp_b200.so"
 
 FP64, FP32_MIXED = 0, 1
+OBSERVE_CURRENT, OBSERVE_GHOST_LAG = 0, 1
 NVE, NOSE_HOOVER, LANGEVIN = 0, 1, 2
 
 STATUS_NAMES = {
@@ -125,6 +126,7 @@ SIGNATURES = {
     "mdg_calculate": (ctypes.c_int, [_H, ctypes.c_int]),
     "mdg_forces": (ctypes.c_int, [_H, _DP]),
     "mdg_observe": (ctypes.c_int, [_H, _DP, _DP, _DP]),
+    "mdg_set_observer_mode": (ctypes.c_int, [_H, ctypes.c_int]),
     "mdg_get_pairs": (ctypes.c_int, [_H, _IP, _IP, ctypes.c_int64, _I64P]),
     "mdg_get_info": (ctypes.c_int, [_H, ctypes.POINTER(Info)]),
     "mdg_stream": (ctypes.c_void_p, [_H]),
@@ -339,6 +341,9 @@ class System:
         part = np.empty(cnt.value, dtype=np.int32)
         self._check(self.lib.mdg_get_list(self.h, _i(rows), _i(part), cnt.value, ctypes.byref(cnt)))
         return rows, part
+
+    def set_observer_mode(self, mode: int):
+        self._check(self.lib.mdg_set_observer_mode(self.h, int(mode)))
 
     def zeta(self) -> float:
         z = ctypes.c_double()

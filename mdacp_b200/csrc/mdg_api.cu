@@ -44,6 +44,8 @@ struct mdg_handle {
   bool graph_dirty = true;
   bool timing = false;
   bool use_graphs = true;
+  int observer_mode = 0;              // MDG_OBSERVE_CURRENT or MDG_OBSERVE_GHOST_LAG
+  double obs_lag = 0.0;               // half-step lag of the reference's ghost copies, when it applies
   std::vector<cudaEvent_t> ev;        // force-kernel start/stop per step of the graph
   double force_ms = 0.0;
   int64_t force_launches = 0;
@@ -73,7 +75,7 @@ cudaError_t dalloc(T **p, size_t count) {
 }
 
 void free_arrays(Arrays &a) {
-  void *ptrs[] = {a.q, a.v, a.q_old, a.qfix, a.ids, a.type, a.cell, a.nbr, a.nnbr, a.cell_count,
+  void *ptrs[] = {a.q, a.v, a.q_old, a.qfix, a.qloc, a.ids, a.type, a.cell, a.nbr, a.nnbr, a.cell_count,
                   a.cell_start, a.slot, a.perm, a.perm2, a.q_tmp, a.v_tmp, a.ids_tmp, a.type_tmp,
                   a.cell_tmp, a.mult, a.cand, a.partials, a.st};
   for (void *p : ptrs)
@@ -490,6 +492,10 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   b.rc2f = (float)b.rc2;
   b.c2x8f = (float)(b.c2 * 8.0);
   b.check_list_length = prm->check_list_length;
+  for (int d = 0; d < 3; d++) b.cs[d] = prm->L[d] / (double)b.ms[d];
+  // FP32 prefilter band: FP32 r^2 within 1e-4 SL^2 of SL^2 is decided in FP64
+  b.sl2_lo = (float)(b.sl2 * (1.0 - 1e-4));
+  b.sl2_hi = (float)(b.sl2 * (1.0 + 1e-4));
   h->ncell = b.ncell;
   h->cap = prm->capacity;
 
@@ -512,6 +518,7 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   if (e == cudaSuccess) e = dalloc(&a.v, cap);
   if (e == cudaSuccess) e = dalloc(&a.q_old, cap);
   if (e == cudaSuccess) e = dalloc(&a.qfix, cap);
+  if (e == cudaSuccess) e = dalloc(&a.qloc, cap);
   if (e == cudaSuccess) e = dalloc(&a.ids, cap);
   if (e == cudaSuccess) e = dalloc(&a.type, cap);
   if (e == cudaSuccess) e = dalloc(&a.cell, cap);
@@ -599,6 +606,7 @@ mdg_status mdg_set_state(mdg_handle *h, const double *q4, const double *v4, cons
   CUDA_TRY(h, cudaGetLastError());
   if (n != h->n) h->graph_dirty = true;
   h->n = n;
+  h->obs_lag = 0.0;
   int dev_error = 0;
   CUDA_TRY(h, cudaMemcpyAsync(&dev_error, &h->a.st->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
@@ -643,6 +651,7 @@ mdg_status mdg_particle_number(mdg_handle *h, int *n) {
 mdg_status mdg_make_pairlist(mdg_handle *h) {
   mdg_status r = check_ready(h);
   if (r) return r;
+  h->obs_lag = 0.0;
   if (h->n == 0) return MDG_OK;
   const int one = 1;
   CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->list_stale, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream));
@@ -675,6 +684,7 @@ mdg_status mdg_check_expired(mdg_handle *h, int *expired) {
 mdg_status mdg_update_position_half(mdg_handle *h) {
   mdg_status r = check_ready(h);
   if (r) return r;
+  h->obs_lag = 0.0;
   if (h->n == 0) return MDG_OK;
   launch_drift(h, h->stream, h->prm.precision == MDG_FP32_MIXED, 0);
   CUDA_TRY(h, cudaGetLastError());
@@ -684,6 +694,7 @@ mdg_status mdg_update_position_half(mdg_handle *h) {
 mdg_status mdg_calculate_force(mdg_handle *h) {
   mdg_status r = check_ready(h);
   if (r) return r;
+  h->obs_lag = 0.0;
   if (h->n == 0) return MDG_OK;
   if ((r = ensure_list(h))) return r;
   if (h->prm.precision == MDG_FP32_MIXED)
@@ -709,6 +720,7 @@ mdg_status mdg_heatbath_zeta(mdg_handle *h, double t) {
 mdg_status mdg_heatbath_momenta(mdg_handle *h) {
   mdg_status r = check_ready(h);
   if (r) return r;
+  h->obs_lag = 0.0;
   if (h->n == 0) return MDG_OK;
   k_scale_v<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->n, h->prm.time_step * 0.5);
   CUDA_TRY(h, cudaGetLastError());
@@ -718,6 +730,7 @@ mdg_status mdg_heatbath_momenta(mdg_handle *h) {
 mdg_status mdg_langevin(mdg_handle *h) {
   mdg_status r = check_ready(h);
   if (r) return r;
+  h->obs_lag = 0.0;
   if (h->n == 0) return MDG_OK;
   k_langevin<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n, thermo_of(h));
   CUDA_TRY(h, cudaGetLastError());
@@ -828,6 +841,9 @@ mdg_status mdg_calculate(mdg_handle *h, int nsteps) {
     if (st.error) return translate_device_error(h, st);
   }
   if (st.steps < target) return fail(h, MDG_ERR_CAPACITY, "could not complete the steps");
+  // after a full step the reference's ghost copies date from the first half
+  // drift; the Langevin branch has no second drift (src/mdmanager.cc:289-315)
+  h->obs_lag = h->prm.thermostat == MDG_LANGEVIN ? 0.0 : 0.5 * h->prm.time_step;
   return MDG_OK;
 }
 
@@ -853,7 +869,8 @@ mdg_status mdg_observe(mdg_handle *h, double *ke, double *pe, double *virial) {
   if (h->n > 0) {
     if ((r = ensure_list(h))) return r;
     const int nb = blocks_for(h->n, kBlock);
-    k_observe<kBlock><<<nb, kBlock, 0, h->stream>>>(h->a, h->box, h->n);
+    const double lag = h->observer_mode ? h->obs_lag : 0.0;
+    k_observe<kBlock><<<nb, kBlock, 0, h->stream>>>(h->a, h->box, h->n, lag);
     k_final_sum<256, 3><<<1, 256, 0, h->stream>>>(h->a.partials, nb, h->d_sums);
     CUDA_TRY(h, cudaGetLastError());
     CUDA_TRY(h, cudaMemcpyAsync(out, h->d_sums, sizeof out, cudaMemcpyDeviceToHost, h->stream));
@@ -862,6 +879,12 @@ mdg_status mdg_observe(mdg_handle *h, double *ke, double *pe, double *virial) {
   if (ke) *ke = out[0];
   if (pe) *pe = out[1];
   if (virial) *virial = out[2] / 3.0;
+  return MDG_OK;
+}
+
+mdg_status mdg_set_observer_mode(mdg_handle *h, int mode) {
+  if (!h || (mode != MDG_OBSERVE_CURRENT && mode != MDG_OBSERVE_GHOST_LAG)) return MDG_ERR_INVALID_ARGUMENT;
+  h->observer_mode = mode;
   return MDG_OK;
 }
 

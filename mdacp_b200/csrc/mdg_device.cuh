@@ -11,7 +11,11 @@
 //                            displacement in units of L/2^32 (no shift tables)
 //   nbr       int32[maxnb][stride]  full Verlet list, column-major: entry k
 //                            of atom i at nbr[k*stride + i] (coalesced per warp)
-//   nnbr      int32[cap]     row lengths
+//   nnbr      int32[cap]     row lengths; rows are padded with the atom's own
+//                            index up to a multiple of 4 (the FP32 force loop
+//                            walks 4 partners at a time; a self entry has r = 0
+//                            and is masked)
+//   qloc      float4[cap]    cell-local FP32 coordinates at the last build
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -41,6 +45,8 @@ struct Box {
   float rc2f;
   float c2x8f;
   int check_list_length;
+  double cs[3];        // cell size L / ms
+  float sl2_lo, sl2_hi;  // FP32 prefilter band around SearchLength^2
 };
 
 // Mutable device-side state of one handle.
@@ -67,6 +73,7 @@ struct Status {
 struct Arrays {
   double4 *q, *v, *q_old;
   int4 *qfix;
+  float4 *qloc;       // cell-local FP32 coordinates at the last build (list prefilter)
   int *ids, *type;
   int *cell;          // cell of each slot at the last build
   int *nbr, *nnbr;
@@ -444,56 +451,82 @@ __global__ void __launch_bounds__(BLOCK) k_permute(Arrays a, Box b, int n) {
     const double x[3] = {q.x, q.y, q.z};
     m = image_multiplicity(x, b);
     a.mult[s] = (unsigned char)m;
+    // cell-local FP32 coordinates for the list prefilter
+    const int c = a.cell_tmp[s];
+    const int cx = c % b.ms[0], cy = (c / b.ms[0]) % b.ms[1], cz = c / (b.ms[0] * b.ms[1]);
+    a.qloc[s] = make_float4((float)(q.x - cx * b.cs[0]), (float)(q.y - cy * b.cs[1]),
+                            (float)(q.z - cz * b.cs[2]), 0.f);
   }
   const int tot = __reduce_add_sync(0xffffffffu, m);
   if ((threadIdx.x & 31) == 0 && tot) atomicAdd((unsigned long long *)&a.st->total_images, (unsigned long long)tot);
 }
 
+// Exact test of one candidate, the reference's arithmetic
+// (MeshList::SearchMesh, src/meshlist.cc:276-289): ghost image q_j + diff
+// first, then dx = x_i - image, then ((dx*dx + dy*dy) + dz*dz), each
+// operation separately rounded; kept when r^2 <= SearchLength^2.
+__device__ __forceinline__ bool within_search_exact(const double4 &qi, const double4 &qj, double sx, double sy,
+                                                    double sz, double sl2) {
+  const double gx = dadd(qj.x, sx), gy = dadd(qj.y, sy), gz = dadd(qj.z, sz);
+  const double ex = dsub(qi.x, gx), ey = dsub(qi.y, gy), ez = dsub(qi.z, gz);
+  const double r2 = dadd(dadd(dmul(ex, ex), dmul(ey, ey)), dmul(ez, ez));
+  return !(r2 > sl2);
+}
+
 // Rebuild 6/6: full Verlet list.  One thread per atom walks the 27 cells
-// around its own (periodic, >= 3 cells per axis so they are distinct) and
-// keeps partner j when r^2 <= SearchLength^2 with r^2 formed exactly as
-// MeshList::SearchMesh does (src/meshlist.cc:276-289): the ghost image
-// q_j + diff first, then dx = x_i - image, then ((dx*dx + dy*dy) + dz*dz),
-// each operation rounded separately.  Row order: cells in (dz,dy,dx) order,
-// slots ascending.
+// around its own (periodic, >= 3 cells per axis so they are distinct).  Each
+// candidate is first tested in FP32 on cell-local coordinates (one FADD per
+// axis: the neighbour cell's offset is folded into a per-cell base); only
+// candidates whose FP32 r^2 falls in a thin band around SearchLength^2 --
+// wider than the FP32 error by a factor of about 40 -- are decided by the
+// exact FP64 test, so the pair set is the reference's bit for bit.  Row
+// order: cells in (dz,dy,dx) order, slots ascending; rows padded with the
+// atom's own index to a multiple of 4.
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
   const int i = blockIdx.x * BLOCK + threadIdx.x;
   int cnt = 0;
   if (i < n && !a.st->error) {
-  const double4 qi = a.q[i];
-  const int c = a.cell_tmp[i];
-  const int cx = c % b.ms[0], cy = (c / b.ms[0]) % b.ms[1], cz = c / (b.ms[0] * b.ms[1]);
-  const int maxnb = a.maxnb, stride = a.stride;
-  for (int dz = -1; dz <= 1; dz++) {
-    int z = cz + dz;
-    double sz = 0.0;
-    if (z < 0) { z += b.ms[2]; sz = -b.L[2]; } else if (z >= b.ms[2]) { z -= b.ms[2]; sz = b.L[2]; }
-    for (int dy = -1; dy <= 1; dy++) {
-      int y = cy + dy;
-      double sy = 0.0;
-      if (y < 0) { y += b.ms[1]; sy = -b.L[1]; } else if (y >= b.ms[1]) { y -= b.ms[1]; sy = b.L[1]; }
-      for (int dx = -1; dx <= 1; dx++) {
-        int x = cx + dx;
-        double sx = 0.0;
-        if (x < 0) { x += b.ms[0]; sx = -b.L[0]; } else if (x >= b.ms[0]) { x -= b.ms[0]; sx = b.L[0]; }
-        const int nc = (z * b.ms[1] + y) * b.ms[0] + x;
-        const int beg = a.cell_start[nc], end = a.cell_start[nc + 1];
-        for (int j = beg; j < end; j++) {
-          if (j == i) continue;
-          const double4 qj = a.q[j];
-          const double gx = dadd(qj.x, sx), gy = dadd(qj.y, sy), gz = dadd(qj.z, sz);
-          const double ex = dsub(qi.x, gx), ey = dsub(qi.y, gy), ez = dsub(qi.z, gz);
-          const double r2 = dadd(dadd(dmul(ex, ex), dmul(ey, ey)), dmul(ez, ez));
-          if (r2 > b.sl2) continue;
-          if (cnt < maxnb) a.nbr[(size_t)cnt * stride + i] = j;
-          cnt++;
+    const float4 li = a.qloc[i];
+    const int c = a.cell_tmp[i];
+    const int cx = c % b.ms[0], cy = (c / b.ms[0]) % b.ms[1], cz = c / (b.ms[0] * b.ms[1]);
+    const int maxnb = a.maxnb, stride = a.stride;
+    const float lo = b.sl2_lo, hi = b.sl2_hi;
+    for (int dz = -1; dz <= 1; dz++) {
+      int z = cz + dz;
+      double sz = 0.0;
+      if (z < 0) { z += b.ms[2]; sz = -b.L[2]; } else if (z >= b.ms[2]) { z -= b.ms[2]; sz = b.L[2]; }
+      const float bz = (float)((z - cz) * b.cs[2] + sz) - li.z;
+      for (int dy = -1; dy <= 1; dy++) {
+        int y = cy + dy;
+        double sy = 0.0;
+        if (y < 0) { y += b.ms[1]; sy = -b.L[1]; } else if (y >= b.ms[1]) { y -= b.ms[1]; sy = b.L[1]; }
+        const float by = (float)((y - cy) * b.cs[1] + sy) - li.y;
+        for (int dx = -1; dx <= 1; dx++) {
+          int x = cx + dx;
+          double sx = 0.0;
+          if (x < 0) { x += b.ms[0]; sx = -b.L[0]; } else if (x >= b.ms[0]) { x -= b.ms[0]; sx = b.L[0]; }
+          const float bx = (float)((x - cx) * b.cs[0] + sx) - li.x;
+          const int nc = (z * b.ms[1] + y) * b.ms[0] + x;
+          const int beg = a.cell_start[nc], end = a.cell_start[nc + 1];
+          for (int j = beg; j < end; j++) {
+            const float4 lj = a.qloc[j];
+            const float ex = lj.x + bx, ey = lj.y + by, ez = lj.z + bz;
+            const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+            if (r2 > hi || j == i) continue;
+            if (r2 >= lo && !within_search_exact(a.q[i], a.q[j], sx, sy, sz, b.sl2)) continue;
+            if (cnt < maxnb) a.nbr[(size_t)cnt * stride + i] = j;
+            cnt++;
+          }
         }
       }
     }
-  }
-  a.nnbr[i] = min(cnt, maxnb);
-  if (cnt > maxnb) atomicOr(&a.st->error, kErrCapacity);
+    a.nnbr[i] = min(cnt, maxnb);
+    if (cnt > maxnb) {
+      atomicOr(&a.st->error, kErrCapacity);
+    } else {
+      for (int k = cnt; k < ((cnt + 3) & ~3); k++) a.nbr[(size_t)k * stride + i] = i;
+    }
   }
   const int wmax = __reduce_max_sync(0xffffffffu, cnt);
   const int wsum = __reduce_add_sync(0xffffffffu, cnt);
@@ -665,62 +698,79 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp64(Arrays a, Box b, int n, Th
   }
 }
 
+// FP32 reciprocal on the special-function unit (rcp.approx.ftz.f32, PTX ISA):
+// relative error at most one unit in the last place, well inside the FP32
+// force error budget.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // One FP32 pair term from fixed-point positions: the wrapped int32
-// difference is the minimum-image displacement in units of L/2^32.
-// `valid` masks padding lanes of the unrolled loop.
-__device__ __forceinline__ void lj_pair_fp32(const int4 &pi, const int4 &pj, bool valid, float sx, float sy,
-                                             float sz, float rc2, float c2x8, float &fx, float &fy, float &fz) {
+// difference is the minimum-image displacement in units of L/2^32.  r^2 = 0
+// (the padding entries, the atom itself) contributes nothing: the unsigned
+// compare of the float bits keeps 0 < r^2 <= rc^2 in one test.
+__device__ __forceinline__ void lj_pair_fp32(const int4 &pi, const int4 &pj, float sx, float sy, float sz,
+                                             unsigned rc2_bits, float c2x8, float &fx, float &fy, float &fz) {
   const float dx = (float)(pj.x - pi.x) * sx;
   const float dy = (float)(pj.y - pi.y) * sy;
   const float dz = (float)(pj.z - pi.z) * sz;
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float ir2 = __frcp_rn(r2);
+  const float ir2 = rcp_approx(r2);
   const float ir6 = ir2 * ir2 * ir2;
   float df = fmaf(ir2 * ir6, fmaf(-48.f, ir6, 24.f), c2x8);
-  df = (valid && r2 <= rc2) ? df : 0.f;
+  df = (__float_as_uint(r2) - 1u < rc2_bits) ? df : 0.f;
   fx = fmaf(df, dx, fx);
   fy = fmaf(df, dy, fy);
   fz = fmaf(df, dz, fz);
 }
 
 // FP32-mixed force kick.  Displacements come from the fixed-point copy (no
-// ghost atoms, no shift codes).  The row is walked four partners at a time
-// with the next four indices loaded ahead; FP32 partial sums over 8 partners
-// are folded into an FP64 per-atom sum; the kick is FP64.  With DRIFT the
-// second half drift q += v dt/2 and the |v| maximum of the step are done in
-// the same pass: this kernel reads only the fixed-point copy, so moving q
-// here races with no other thread.
+// ghost atoms, no shift codes).  Rows are padded to a multiple of 4, so the
+// row is walked four partners at a time without per-lane masks, with the
+// next four indices loaded ahead; FP32 partial sums over 8 partners are
+// folded into an FP64 per-atom sum; the kick is FP64.  With DRIFT the second
+// half drift q += v dt/2 and the |v| maximum of the step are done in the
+// same pass: this kernel reads only the fixed-point copy, so moving q here
+// races with no other thread.
 template <int BLOCK, int MODE, bool DRIFT>
 __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Thermo th) {
   const int i = blockIdx.x * BLOCK + threadIdx.x;
   double v2 = 0.0, ke = 0.0;
   if (i < n && !a.st->error) {
     const int4 pi = a.qfix[i];
-    const int nn = a.nnbr[i];
+    const int nn4 = (a.nnbr[i] + 3) & ~3;
     const float sx = b.fix_scale[0], sy = b.fix_scale[1], sz = b.fix_scale[2];
-    const float rc2 = b.rc2f, c2x8 = b.c2x8f;
+    const unsigned rc2_bits = __float_as_uint(b.rc2f);
+    const float c2x8 = b.c2x8f;
     const int *row = a.nbr + i;
-    const size_t st = (size_t)a.stride;
+    const int st = a.stride;
     double Fx = 0.0, Fy = 0.0, Fz = 0.0;
     float fx = 0.f, fy = 0.f, fz = 0.f;
-    int n0 = (0 < nn) ? __ldg(row) : i;
-    int n1 = (1 < nn) ? __ldg(row + st) : i;
-    int n2 = (2 < nn) ? __ldg(row + 2 * st) : i;
-    int n3 = (3 < nn) ? __ldg(row + 3 * st) : i;
-    for (int k = 0; k < nn; k += 4) {
-      const int j0 = n0, j1 = n1, j2 = n2, j3 = n3;
-      n0 = (k + 4 < nn) ? __ldg(row + (size_t)(k + 4) * st) : i;
-      n1 = (k + 5 < nn) ? __ldg(row + (size_t)(k + 5) * st) : i;
-      n2 = (k + 6 < nn) ? __ldg(row + (size_t)(k + 6) * st) : i;
-      n3 = (k + 7 < nn) ? __ldg(row + (size_t)(k + 7) * st) : i;
-      const int4 p0 = __ldg(a.qfix + j0);
-      const int4 p1 = __ldg(a.qfix + j1);
-      const int4 p2 = __ldg(a.qfix + j2);
-      const int4 p3 = __ldg(a.qfix + j3);
-      lj_pair_fp32(pi, p0, true, sx, sy, sz, rc2, c2x8, fx, fy, fz);
-      lj_pair_fp32(pi, p1, k + 1 < nn, sx, sy, sz, rc2, c2x8, fx, fy, fz);
-      lj_pair_fp32(pi, p2, k + 2 < nn, sx, sy, sz, rc2, c2x8, fx, fy, fz);
-      lj_pair_fp32(pi, p3, k + 3 < nn, sx, sy, sz, rc2, c2x8, fx, fy, fz);
+    int n0 = i, n1 = i, n2 = i, n3 = i;
+    if (nn4 > 0) {
+      n0 = __ldg(row);
+      n1 = __ldg(row + st);
+      n2 = __ldg(row + 2 * st);
+      n3 = __ldg(row + 3 * st);
+    }
+    for (int k = 0; k < nn4; k += 4) {
+      const int4 p0 = __ldg(a.qfix + n0);
+      const int4 p1 = __ldg(a.qfix + n1);
+      const int4 p2 = __ldg(a.qfix + n2);
+      const int4 p3 = __ldg(a.qfix + n3);
+      if (k + 4 < nn4) {
+        const int *r = row + (size_t)(k + 4) * st;
+        n0 = __ldg(r);
+        n1 = __ldg(r + st);
+        n2 = __ldg(r + 2 * st);
+        n3 = __ldg(r + 3 * st);
+      }
+      lj_pair_fp32(pi, p0, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
+      lj_pair_fp32(pi, p1, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
+      lj_pair_fp32(pi, p2, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
+      lj_pair_fp32(pi, p3, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
       if (k & 4) {
         Fx += (double)fx;
         Fy += (double)fy;
@@ -788,9 +838,13 @@ __global__ void __launch_bounds__(BLOCK) k_zeta(Arrays a, Box b, int nblocks, in
 
 // Observers: KE, PE, virial per atom over the full list, x 1/2 for pair sums
 // (PotentialEnergyObserver / VirialObserver, src/observer.cc:17-79: each
-// pair term formed as the reference forms it).
+// pair term formed as the reference forms it).  lag > 0 reproduces what the
+// reference's observers see after a full NVE or Nose-Hoover step: a partner
+// reached through the periodic boundary is a ghost copy refreshed after the
+// first half drift (MDManager::SendBorderParticles, src/mdmanager.cc:165-167),
+// i.e. the partner's position lag = dt/2 earlier, q_j - v_j dt/2.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_observe(Arrays a, Box b, int n) {
+__global__ void __launch_bounds__(BLOCK) k_observe(Arrays a, Box b, int n, double lag) {
   const int i = blockIdx.x * BLOCK + threadIdx.x;
   double ke = 0.0, pe = 0.0, vir = 0.0;
   if (i < n) {
@@ -800,7 +854,14 @@ __global__ void __launch_bounds__(BLOCK) k_observe(Arrays a, Box b, int n) {
     const int nn = a.nnbr[i];
     for (int k = 0; k < nn; k++) {
       const int j = a.nbr[(size_t)k * a.stride + i];
-      const double4 qj = a.q[j];
+      double4 qj = a.q[j];
+      if (lag > 0.0 && (fabs(qj.x - qi.x) > b.hL[0] || fabs(qj.y - qi.y) > b.hL[1] ||
+                        fabs(qj.z - qi.z) > b.hL[2])) {
+        const double4 vj = a.v[j];
+        qj.x = dsub(qj.x, dmul(vj.x, lag));
+        qj.y = dsub(qj.y, dmul(vj.y, lag));
+        qj.z = dsub(qj.z, dmul(vj.z, lag));
+      }
       const double dx = dsub(qi.x, image_of(qj.x, qi.x, b.L[0], b.hL[0]));
       const double dy = dsub(qi.y, image_of(qj.y, qi.y, b.L[1], b.hL[1]));
       const double dz = dsub(qi.z, image_of(qj.z, qi.z, b.L[2], b.hL[2]));

@@ -57,6 +57,8 @@ void MDUnit::CreateDevice(void) {
   prm.seed = static_cast<uint64_t>(id);
   mdg_handle *h = nullptr;
   mdg_check(nullptr, mdg_create(&prm, &h), "mdg_create");
+  // observers see the reference's half-step-old ghost copies (see mdacp_b200.h)
+  mdg_check(h, mdg_set_observer_mode(h, MDG_OBSERVE_GHOST_LAG), "mdg_set_observer_mode");
   dev = h;
   vars->AttachDevice(dev);
   mesh->Attach(vars);

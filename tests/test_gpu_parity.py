@@ -81,6 +81,27 @@ def test_trajectory_fp64_matches_reference(golden):
     assert abs(info["rebuilds"] - int(golden["constructions"])) <= 2
 
 
+def test_observers_along_trajectory_match_reference(golden):
+    # the reference's KE/N, PE/N and virial every steps/4 steps; its
+    # observers see ghost copies half a step old (MDG_OBSERVE_GHOST_LAG)
+    nh = str(golden["thermostat"]) == "NoseHoover"
+    kw = {}
+    if nh:
+        kw = dict(thermostat=M.NOSE_HOOVER, aimed_temperature=float(golden["aimed_temperature"]),
+                  heatbath_tau=float(golden["heatbath_tau"]))
+    s = gsys(golden, **kw)
+    s.set_observer_mode(M.OBSERVE_GHOST_LAG)
+    n = golden["q"].shape[0]
+    every = max(1, int(golden["steps"]) // 4)
+    assert golden["traj_obs"].shape[0] == 4
+    for row in golden["traj_obs"]:
+        s.calculate(every)
+        ke, pe, vir = s.observe()
+        assert ke / n == pytest.approx(row[0], rel=1e-9)
+        assert pe / n == pytest.approx(row[1], rel=1e-9)
+        assert vir == pytest.approx(row[2], rel=1e-9)
+
+
 @pytest.mark.parametrize("rho,temperature", [(0.5, 1.0), (0.8442, 1.0)])
 def test_matches_oracle_32k(rho, temperature):
     # 32,000 atoms at the densities of the 32k workloads; the lattice is
