@@ -155,7 +155,7 @@ def local_grid(t, L, sl):
     return best[1] if best else None
 
 
-def run_reference_bench(state, steps, warmup, threads):
+def run_reference_bench(state, steps, warmup, threads, config):
     """Times the reference's own CPU build (AVX2, oracle/_ref) on the state
     through its OracleBench project; returns (atom_steps_per_s, info)."""
     from oracle import lj_oracle as O
@@ -167,6 +167,9 @@ def run_reference_bench(state, steps, warmup, threads):
         grid = local_grid(t, state.L, state.rc + 0.3)
     extra = {"Steps": str(steps), "Warmup": str(warmup), "LocalGridX": str(grid[0]),
              "LocalGridY": str(grid[1]), "LocalGridZ": str(grid[2])}
+    if config.get("thermostat") == "Langevin":
+        extra.update(ControlTemperature="yes", HeatbathType="Langevin",
+                     AimedTemperature=repr(config["temperature"]), HeatbathGamma=repr(config["gamma"]))
     wd, out = O.run_reference("OracleBench", state.q, state.v, state.ids, state.L, state.rc, state.dt,
                               flavour="avx2", threads=t, extra=extra, timeout=1800)
     line = [x for x in out.splitlines() if x.startswith("ORACLE_BENCH")][-1].split()
@@ -176,10 +179,10 @@ def run_reference_bench(state, steps, warmup, threads):
                                     "rebuilds": int(round(kv["rebuilds"] / kv["units"]))}
 
 
-def ref_sample_steps(cores, seconds):
-    # about 2.6e6 atom-steps/s per core for the AVX2 build at this density
+def ref_sample_steps(cores, seconds, n):
+    # about 2.6e6 atom-steps/s per core for the AVX2 build at rho 0.84, rc 2.5
     est = 2.6e6 * cores
-    return int(min(2000, max(10, seconds * est / 2.048e6)))
+    return int(min(2000, max(10, seconds * est / n)))
 
 
 # -------------------------------------------------------------------- main
@@ -198,35 +201,74 @@ def main():
     ap.add_argument("--no-force-error", action="store_true", help="skip the FP32-vs-FP64 force check")
     ap.add_argument("--eager", action="store_true",
                     help="launch every kernel from the host instead of CUDA graphs (for profilers)")
+    ap.add_argument("--config", choices=["c2", "c1", "c3", "c4"], default="c2",
+                    help="c2: 2.05M-atom liquid (headline); c1: 32k atoms rho 0.5; c3: 1M-atom Langevin slab; "
+                         "c4: 256-replica ensemble")
     args = ap.parse_args()
     ws, rank, local = dist_env()
-    from mdacp_b200 import workloads as W
-
-    state = W.fcc_liquid(args.cells, 0.8442, 0.722, seed=2026 + rank, rc=2.5, dt=0.004,
-                         name=f"lj_fcc{4 * args.cells ** 3}_rho0.8442")
-    n = state.n
-    config = {
-        "workload": f"{state.name}: {n} atoms, FCC {args.cells}^3 cells, rho 0.8442, L {state.L[0]:.4f}, "
-                    "T 0.722, rc 2.5, search length 2.8, dt 0.004, NVE",
-        "n_atoms": n, "rho": 0.8442, "temperature": 0.722, "rc": 2.5, "search_length": 2.8, "dt": 0.004,
-        "md_steps_per_step": args.md_steps_per_step,
-        "l2": "inputs larger than L2 (state 131 MB + pairlist > 1 GB per replica)",
-        "parallelism": "replicas" if args.gpus > 1 else "single",
-    }
+    if args.config == "c4":
+        return main_ensemble(args, ws, rank, local)
+    state, config = workload(args, rank)
     if args.impl == "reference":
         return main_reference(args, ws, rank, state, config)
     return main_mdg(args, ws, rank, local, state, config)
+
+
+def workload(args, rank):
+    """The synthetic state and the JSON config of the selected workload."""
+    from mdacp_b200 import workloads as W
+
+    common = {"md_steps_per_step": args.md_steps_per_step,
+              "parallelism": "replicas" if args.gpus > 1 else "single"}
+    if args.config == "c1":
+        state = W.config_c1(seed=12345 + rank)
+        config = dict(common, workload=f"{state.name}: {state.n} atoms, FCC 20^3 cells, rho 0.5, L 40, T 1.0, "
+                                      "rc 2.5, search length 2.8, dt 0.005, NVE",
+                      n_atoms=state.n, rho=0.5, temperature=1.0, rc=2.5, search_length=2.8, dt=0.005,
+                      thermostat="NVE", l2="small system: state (2 MB) and list (6 MB) stay L2-resident")
+        return state, config
+    if args.config == "c3":
+        state = W.config_c3(seed=31 + rank)
+        config = dict(common, workload=f"{state.name}: {state.n} atoms, 1:1:4 box {state.L[0]:.2f}^2 x "
+                                      f"{state.L[2]:.2f}, liquid slab rho 0.75 in the middle quarter, vapour "
+                                      "rho 0.02, overlaps < 0.9 rejected, T 0.9, Langevin gamma 1.0 (Philox "
+                                      "noise), rc 3.0, search length 3.3, dt 0.005",
+                      n_atoms=state.n, temperature=0.9, rc=3.0, search_length=3.3, dt=0.005,
+                      thermostat="Langevin", gamma=1.0,
+                      l2="inputs larger than L2 (state 64 MB + pairlist > 400 MB)")
+        return state, config
+    state = W.fcc_liquid(args.cells, 0.8442, 0.722, seed=2026 + rank, rc=2.5, dt=0.004,
+                         name=f"lj_fcc{4 * args.cells ** 3}_rho0.8442")
+    config = dict(common, workload=f"{state.name}: {state.n} atoms, FCC {args.cells}^3 cells, rho 0.8442, "
+                                  f"L {state.L[0]:.4f}, T 0.722, rc 2.5, search length 2.8, dt 0.004, NVE",
+                  n_atoms=state.n, rho=0.8442, temperature=0.722, rc=2.5, search_length=2.8, dt=0.004,
+                  thermostat="NVE", l2="inputs larger than L2 (state 131 MB + pairlist > 1 GB per replica)")
+    return state, config
+
+
+def metric_for(config):
+    if config["n_atoms"] == 2048000 and config.get("thermostat") == "NVE":
+        return METRIC
+    return f"LJ atom-steps/s, {config['workload'].split(':')[0]}"
+
+
+def system_kwargs(state, config, M):
+    kw = dict(cutoff=state.rc, time_step=state.dt, capacity=state.n)
+    if config.get("thermostat") == "Langevin":
+        kw.update(thermostat=M.LANGEVIN, aimed_temperature=config["temperature"],
+                  heatbath_gamma=config["gamma"], seed=7)
+    return kw
 
 
 def main_reference(args, ws, rank, state, config):
     if rank != 0:
         return 0
     cores = ref_threads()
-    md_steps = ref_sample_steps(cores, 60.0)
-    value, info = run_reference_bench(state, md_steps, max(1, min(args.warmup, 5)), cores)
+    md_steps = ref_sample_steps(cores, 60.0, state.n)
+    value, info = run_reference_bench(state, md_steps, max(1, min(args.warmup, 5)), cores, config)
     ms_per_md = 1e3 * state.n / value
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": info["steps"],
+        "metric": metric_for(config), "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": info["steps"],
         "warmup": max(1, min(args.warmup, 5)), "ms_per_step": ms_per_md, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
         "config": dict(config, md_steps_per_step=1, precision="fp64 (reference AVX2 CPU build)",
@@ -292,7 +334,7 @@ def main_mdg(args, ws, rank, local, state, config):
     if args.precision != "both":
         runs = [r for r in runs if r[0] == args.precision]
     for prec_name, prec in runs:
-        s = M.System(state.L, cutoff=state.rc, time_step=state.dt, capacity=n, precision=prec, device=local)
+        s = M.System(state.L, precision=prec, device=local, **system_kwargs(state, config, M))
         s.set_state(state.q, state.v)
         if args.eager:
             s.set_graph_mode(False)
@@ -303,8 +345,10 @@ def main_mdg(args, ws, rank, local, state, config):
             clocks = sampler.stop()
         ms_max = max_over_ranks(dist, ms, device)
         md_steps = args.steps * args.md_steps_per_step
+        within, _ = s.pair_counts()
         result[prec_name] = dict(ms=ms_max, value=ws * n * md_steps / (ms_max * 1e-3), force_ms=fms,
-                                 force_launches=flaunch, launches=launches, info0=info0, info1=info1)
+                                 force_launches=flaunch, launches=launches, info0=info0, info1=info1,
+                                 pairs=within // 2)
         s.close()
 
     if args.precision != "both" or args.no_e2e or args.no_force_error:
@@ -318,7 +362,7 @@ def main_mdg(args, ws, rank, local, state, config):
         return 0
 
     # end to end through the C ABI from pinned host buffers (FP32-mixed path)
-    s = M.System(state.L, cutoff=state.rc, time_step=state.dt, capacity=n, precision=M.FP32_MIXED, device=local)
+    s = M.System(state.L, precision=M.FP32_MIXED, device=local, **system_kwargs(state, config, M))
     hq = torch.empty((n, 4), dtype=torch.float64, pin_memory=True).numpy()
     hv = torch.empty((n, 4), dtype=torch.float64, pin_memory=True).numpy()
     hq[:, :3] = state.q
@@ -342,13 +386,13 @@ def main_mdg(args, ws, rank, local, state, config):
 
     # FP32-mixed force error against FP64 at full size
     errs = {}
-    sa = M.System(state.L, cutoff=state.rc, time_step=state.dt, capacity=n, precision=M.FP64, device=local)
+    sa = M.System(state.L, precision=M.FP64, device=local, **system_kwargs(state, config, M))
     sa.set_state(state.q, state.v)
     sa.calculate(50)
     q, v = sa.state_by_id()
     f64 = sa.forces_by_id()
     sa.close()
-    sb = M.System(state.L, cutoff=state.rc, time_step=state.dt, capacity=n, precision=M.FP32_MIXED, device=local)
+    sb = M.System(state.L, precision=M.FP32_MIXED, device=local, **system_kwargs(state, config, M))
     sb.set_state(q, v)
     f32 = sb.forces_by_id()
     sb.close()
@@ -370,7 +414,7 @@ def main_mdg(args, ws, rank, local, state, config):
     if prof.exists():
         traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
     line = {
-        "metric": METRIC, "value": r32["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "metric": metric_for(config), "value": r32["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r32["ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": dict(config, precision="fp32_mixed: FP32 pair forces on fixed-point minimum-image "
@@ -379,6 +423,10 @@ def main_mdg(args, ws, rank, local, state, config):
         "fp64": {"value": r64["value"], "ms_per_md_step": r64["ms"] / (args.steps * args.md_steps_per_step),
                  "speedup_fp32_over_fp64": r32["value"] / r64["value"]},
         "ms_per_md_step": r32["ms"] / (args.steps * args.md_steps_per_step),
+        "pair_interactions_per_s": {
+            "fp32": ws * r32["pairs"] * args.steps * args.md_steps_per_step / (r32["ms"] * 1e-3),
+            "fp64": ws * r64["pairs"] * args.steps * args.md_steps_per_step / (r64["ms"] * 1e-3),
+            "pairs_within_cutoff_per_step": r32["pairs"]},
         "force_error_fp32_vs_fp64": errs,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "kernel": "k_force_fp32 (kick)",
@@ -392,13 +440,83 @@ def main_mdg(args, ws, rank, local, state, config):
     if rank == 0 and not args.no_cpu_baseline and ws == 1:
         try:
             cores = ref_threads()
-            v, info = run_reference_bench(state, ref_sample_steps(cores, 15.0), 2, cores)
+            v, info = run_reference_bench(state, ref_sample_steps(cores, 15.0, n), 2, cores, config)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "reference",
                                     "sample": f"{info['steps']} MD steps of the same {n}-atom system, "
                                               f"reference AVX2 build, {info['sec']:.2f} s"}
         except Exception as exc:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                                     "sample": f"not run: {exc}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main_ensemble(args, ws, rank, local):
+    """256 independent replicas (N 500-20000, rho 0.3-0.9, T 0.7-1.5, jittered
+    FCC) in one mdg_ensemble, FP32-mixed, against looping the single-system
+    handle over the same replicas."""
+    import torch
+
+    import mdacp_b200 as M
+    from mdacp_b200 import workloads as W
+
+    dist = init_dist(ws, "nccl")
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    reps = W.config_c4(seed=404 + rank)
+    ntot = sum(r.n for r in reps)
+    mdn = args.md_steps_per_step
+    ens = M.Ensemble([(r.q, r.v, r.L) for r in reps], cutoff=2.5, time_step=0.005, precision=M.FP32_MIXED,
+                     device=local)
+    for _ in range(args.warmup):
+        ens.calculate(mdn)
+    stream = torch.cuda.ExternalStream(ens.stream())
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ens.calculate(mdn)
+    e1.record(stream)
+    e1.synchronize()
+    ms = max_over_ranks(dist, e0.elapsed_time(e1), device)
+    value = ws * ntot * args.steps * mdn / (ms * 1e-3)
+    rb, _ = ens.rebuilds()
+    ens.close()
+    # looping the single-system path: one handle per replica, stepped in turn
+    loop_steps = max(20, mdn // 5)
+    systems = []
+    for r in reps:
+        sy = M.System(r.L, cutoff=2.5, time_step=0.005, capacity=r.n, precision=M.FP32_MIXED, device=local)
+        sy.set_state(r.q, r.v)
+        sy.calculate(20)  # first build + graph capture outside the timing
+        systems.append(sy)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for sy in systems:
+        sy.calculate(loop_steps)
+    torch.cuda.synchronize()
+    loop_s = time.perf_counter() - t0
+    loop_value = ntot * loop_steps / loop_s
+    for sy in systems:
+        sy.close()
+    line = {
+        "metric": "LJ atom-steps/s, 256-replica ensemble (N 500-20000)", "value": value, "unit": UNIT,
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"256 replicas, {ntot} atoms in total, N 500-20000, rho 0.3-0.9, T 0.7-1.5, "
+                               "jittered FCC, rc 2.5, search length 2.8, dt 0.005, NVE, FP32-mixed",
+                   "md_steps_per_step": mdn, "replicas": len(reps), "atoms": ntot,
+                   "rebuilds_per_replica_mean": float(np.mean(rb)),
+                   "l2": "inputs larger than L2 (state 160 MB + pairlists)"},
+        "looped_single_system": {"value": loop_value, "unit": UNIT, "md_steps": loop_steps,
+                                 "note": "one handle per replica, calculate() in turn, host wall clock"},
+        "speedup_vs_looped": value / loop_value,
+    }
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

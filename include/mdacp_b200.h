@@ -150,6 +150,11 @@ mdg_status mdg_observe(mdg_handle *h, double *ke, double *pe, double *virial);
    the reference prints. */
 mdg_status mdg_set_observer_mode(mdg_handle *h, int mode);
 
+/* Directed list entries within the cut-off (pair terms one force
+   evaluation computes; unordered pairs = within_cutoff / 2) and all list
+   entries, at the current positions. */
+mdg_status mdg_pair_counts(mdg_handle *h, int64_t *within_cutoff, int64_t *list_entries);
+
 /* Pairlist readout for parity (MeshList::GetPairNumber, GetKeyPointer,
    GetPartnerNumber, GetSortedList, include/meshlist.h:70-91).  Directed
    (key, partner) pairs, expressed as upload indices, one per atom that has
@@ -208,6 +213,35 @@ mdg_status mdg_kernel_time(mdg_handle *h, double *force_ms, int64_t *force_launc
 mdg_status mdg_observe_static(const double *q4, const double *v4, int n, const int *row_start,
                               const int *partners, const double L[3], double cutoff, double *out,
                               void *stream);
+
+/* ---------------------------------------------------------------- ensembles
+   Many independent periodic systems (replicas) of different size, density
+   and temperature advanced together; no counterpart in the reference, which
+   runs one system per MPI job.  Every kernel of a step covers all replicas
+   in one launch (per-replica cell grids and offset tables); each replica
+   keeps its own skin budget and rebuilds only its own list, with the
+   single-system arithmetic, so a replica evolves bit-identically to the
+   same system in its own handle.  NVE only.  Arrays are the replicas'
+   atoms concatenated in replica order, n x 4 doubles. */
+typedef struct mdg_ensemble mdg_ensemble;
+typedef struct {
+  int n;          /* atoms */
+  double L[3];    /* box; every length must exceed 2 x SearchLength */
+} mdg_replica;
+/* common: cutoff, buffer_length, time_step, precision, check_list_length,
+   device (capacity, thermostat and stream are not used). */
+mdg_status mdg_ensemble_create(const mdg_params *common, int nrep, const mdg_replica *replicas,
+                               mdg_ensemble **out);
+mdg_status mdg_ensemble_destroy(mdg_ensemble *e);
+mdg_status mdg_ensemble_set_state(mdg_ensemble *e, const double *q4, const double *v4);
+/* Current slot order; ids (may be NULL) = upload index within the replica. */
+mdg_status mdg_ensemble_get_state(mdg_ensemble *e, double *q4, double *v4, int *ids);
+mdg_status mdg_ensemble_calculate(mdg_ensemble *e, int nsteps);
+/* Per-replica sums (arrays of nrep), as mdg_observe returns them. */
+mdg_status mdg_ensemble_observe(mdg_ensemble *e, double *ke, double *pe, double *virial);
+mdg_status mdg_ensemble_rebuilds(mdg_ensemble *e, int64_t *rebuilds, int64_t *steps);
+mdg_status mdg_ensemble_set_graph_mode(mdg_ensemble *e, int use_graphs);
+void *mdg_ensemble_stream(mdg_ensemble *e);
 
 const char *mdg_last_error(mdg_handle *h);
 const char *mdg_status_string(mdg_status s);

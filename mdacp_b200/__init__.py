@@ -18,7 +18,9 @@ __all__ = [
     "MdgError",
     "Params",
     "Info",
+    "Replica",
     "System",
+    "Ensemble",
     "load_library",
     "FP64",
     "FP32_MIXED",
@@ -99,6 +101,12 @@ class Info(ctypes.Structure):
                 for name, _ in self._fields_}
 
 
+class Replica(ctypes.Structure):
+    """``mdg_replica`` (include/mdacp_b200.h)."""
+
+    _fields_ = [("n", ctypes.c_int), ("L", ctypes.c_double * 3)]
+
+
 # name -> (restype, argtypes)
 _H = ctypes.c_void_p
 _DP = ctypes.POINTER(ctypes.c_double)
@@ -127,6 +135,7 @@ SIGNATURES = {
     "mdg_forces": (ctypes.c_int, [_H, _DP]),
     "mdg_observe": (ctypes.c_int, [_H, _DP, _DP, _DP]),
     "mdg_set_observer_mode": (ctypes.c_int, [_H, ctypes.c_int]),
+    "mdg_pair_counts": (ctypes.c_int, [_H, _I64P, _I64P]),
     "mdg_get_pairs": (ctypes.c_int, [_H, _IP, _IP, ctypes.c_int64, _I64P]),
     "mdg_get_info": (ctypes.c_int, [_H, ctypes.POINTER(Info)]),
     "mdg_stream": (ctypes.c_void_p, [_H]),
@@ -135,6 +144,16 @@ SIGNATURES = {
     "mdg_kernel_time": (ctypes.c_int, [_H, _DP, _I64P, _I64P]),
     "mdg_observe_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                           ctypes.c_void_p, _DP, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]),
+    "mdg_ensemble_create": (ctypes.c_int, [ctypes.POINTER(Params), ctypes.c_int, ctypes.c_void_p,
+                                           ctypes.POINTER(_H)]),
+    "mdg_ensemble_destroy": (ctypes.c_int, [_H]),
+    "mdg_ensemble_set_state": (ctypes.c_int, [_H, _DP, _DP]),
+    "mdg_ensemble_get_state": (ctypes.c_int, [_H, _DP, _DP, _IP]),
+    "mdg_ensemble_calculate": (ctypes.c_int, [_H, ctypes.c_int]),
+    "mdg_ensemble_observe": (ctypes.c_int, [_H, _DP, _DP, _DP]),
+    "mdg_ensemble_rebuilds": (ctypes.c_int, [_H, _I64P, _I64P]),
+    "mdg_ensemble_set_graph_mode": (ctypes.c_int, [_H, ctypes.c_int]),
+    "mdg_ensemble_stream": (ctypes.c_void_p, [_H]),
     "mdg_last_error": (ctypes.c_char_p, [_H]),
     "mdg_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "mdg_version": (ctypes.c_char_p, []),
@@ -342,6 +361,12 @@ class System:
         self._check(self.lib.mdg_get_list(self.h, _i(rows), _i(part), cnt.value, ctypes.byref(cnt)))
         return rows, part
 
+    def pair_counts(self):
+        """(directed list entries within the cut-off, all list entries)."""
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.mdg_pair_counts(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def set_observer_mode(self, mode: int):
         self._check(self.lib.mdg_set_observer_mode(self.h, int(mode)))
 
@@ -370,3 +395,95 @@ class System:
         kl = ctypes.c_int64()
         self._check(self.lib.mdg_kernel_time(self.h, ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(kl)))
         return ms.value, fl.value, kl.value
+
+
+class Ensemble:
+    """Independent periodic replicas advanced together (mdg_ensemble_*).
+    ``states`` is a list of (q, v, L) per replica."""
+
+    def __init__(self, states, cutoff=2.5, time_step=0.005, precision=FP64, buffer_length=0.3,
+                 check_list_length=500, device=0):
+        self.lib = load_library()
+        p = Params()
+        self.lib.mdg_default_params(ctypes.byref(p))
+        p.cutoff = float(cutoff)
+        p.time_step = float(time_step)
+        p.precision = int(precision)
+        p.buffer_length = float(buffer_length)
+        p.check_list_length = int(check_list_length)
+        p.device = int(device)
+        self.nrep = len(states)
+        reps = (Replica * self.nrep)()
+        self.sizes = []
+        for k, (q, v, L) in enumerate(states):
+            reps[k].n = int(q.shape[0])
+            reps[k].L[:] = [float(x) for x in L]
+            self.sizes.append(int(q.shape[0]))
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
+        h = _H()
+        st = self.lib.mdg_ensemble_create(ctypes.byref(p), self.nrep, ctypes.cast(reps, ctypes.c_void_p),
+                                          ctypes.byref(h))
+        if st != 0:
+            raise MdgError(st, self.lib.mdg_status_string(st).decode())
+        self.h = h
+        self.ntot = int(self.offsets[-1])
+        q4 = np.zeros((self.ntot, 4))
+        v4 = np.zeros((self.ntot, 4))
+        for k, (q, v, _) in enumerate(states):
+            a, b = self.offsets[k], self.offsets[k + 1]
+            q4[a:b, :3] = q
+            v4[a:b, :3] = v
+        self._check(self.lib.mdg_ensemble_set_state(self.h, _d(q4), _d(v4)))
+
+    def _check(self, st):
+        if st != 0:
+            raise MdgError(st, self.lib.mdg_status_string(st).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mdg_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def calculate(self, nsteps):
+        self._check(self.lib.mdg_ensemble_calculate(self.h, int(nsteps)))
+
+    def set_graph_mode(self, use_graphs):
+        self._check(self.lib.mdg_ensemble_set_graph_mode(self.h, int(bool(use_graphs))))
+
+    def stream(self):
+        return self.lib.mdg_ensemble_stream(self.h)
+
+    def states_by_id(self):
+        """Per replica (q, v) ordered by upload index within the replica."""
+        q4 = np.empty((self.ntot, 4))
+        v4 = np.empty((self.ntot, 4))
+        ids = np.empty(self.ntot, dtype=np.int32)
+        self._check(self.lib.mdg_ensemble_get_state(self.h, _d(q4), _d(v4), _i(ids)))
+        out = []
+        for k in range(self.nrep):
+            a, b = self.offsets[k], self.offsets[k + 1]
+            q = np.empty((b - a, 3))
+            v = np.empty((b - a, 3))
+            q[ids[a:b]] = q4[a:b, :3]
+            v[ids[a:b]] = v4[a:b, :3]
+            out.append((q, v))
+        return out
+
+    def observe(self):
+        ke = np.empty(self.nrep)
+        pe = np.empty(self.nrep)
+        vir = np.empty(self.nrep)
+        self._check(self.lib.mdg_ensemble_observe(self.h, _d(ke), _d(pe), _d(vir)))
+        return ke, pe, vir
+
+    def rebuilds(self):
+        r = np.empty(self.nrep, dtype=np.int64)
+        s = np.empty(self.nrep, dtype=np.int64)
+        self._check(self.lib.mdg_ensemble_rebuilds(self.h, r.ctypes.data_as(_I64P), s.ctypes.data_as(_I64P)))
+        return r, s

@@ -154,12 +154,19 @@ int estimate_max_neighbors(const mdg_handle *h, const double *q4, int n) {
 
 // ------------------------------------------------------ kernel sequences
 // Displacement check (PairList::CheckByDisplacement).
-void launch_disp(mdg_handle *h, cudaStream_t s) {
+// lag: age of the reference's ghost copies at this check (see for_each_copy).
+void launch_disp(mdg_handle *h, cudaStream_t s, double lag) {
   const int n = h->n;
-  k_disp_max<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(h->a, n);
+  k_disp_max<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(h->a, h->box, n, lag);
   k_disp_collect<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(h->a, h->box, n,
-                                                                   h->prm.check_list_length);
-  k_disp_pairs<1024><<<1, 1024, 0, s>>>(h->a, h->box);
+                                                                   h->prm.check_list_length, lag);
+  k_disp_pairs<1024><<<1, 1024, 0, s>>>(h->a, h->box, lag);
+}
+
+// Ghost age at the skin check of a step: the previous step ended with a half
+// drift after the ghosts were refreshed, except in the Langevin branch.
+double step_lag(const mdg_handle *h) {
+  return h->prm.thermostat == MDG_LANGEVIN ? 0.0 : 0.5 * h->prm.time_step;
 }
 
 // Pairlist rebuild (MDManager::MakePairList).
@@ -327,7 +334,7 @@ mdg_status build_graph(mdg_handle *h) {
     {
       Capture bc{h->cap_stream, body, {}};
       CUDA_TRY(h, begin_capture(bc));
-      launch_disp(h, bc.s);
+      launch_disp(h, bc.s, step_lag(h));
       CUDA_TRY(h, end_capture(bc));
     }
     CUDA_TRY(h, begin_capture(c));
@@ -362,7 +369,7 @@ mdg_status step_eager(mdg_handle *h) {
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   h->kernel_launches++;
   if (flags[0]) {
-    launch_disp(h, h->stream);
+    launch_disp(h, h->stream, step_lag(h));
     h->kernel_launches += 3;
   }
   k_decide<<<1, 32, 0, h->stream>>>(h->a, 0, 0, h->d_flags);
@@ -669,7 +676,7 @@ mdg_status mdg_check_expired(mdg_handle *h, int *expired) {
   k_expiry<<<1, 32, 0, h->stream>>>(h->a, h->box, 0, 0, h->d_flags);
   CUDA_TRY(h, cudaMemcpyAsync(flags, h->d_flags, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  if (flags[0]) launch_disp(h, h->stream);
+  if (flags[0]) launch_disp(h, h->stream, h->obs_lag);
   k_decide<<<1, 32, 0, h->stream>>>(h->a, 0, 0, h->d_flags);
   CUDA_TRY(h, cudaMemcpyAsync(flags, h->d_flags, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
@@ -879,6 +886,24 @@ mdg_status mdg_observe(mdg_handle *h, double *ke, double *pe, double *virial) {
   if (ke) *ke = out[0];
   if (pe) *pe = out[1];
   if (virial) *virial = out[2] / 3.0;
+  return MDG_OK;
+}
+
+mdg_status mdg_pair_counts(mdg_handle *h, int64_t *within_cutoff, int64_t *list_entries) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  unsigned long long c[2] = {0ull, 0ull};
+  if (h->n > 0) {
+    if ((r = ensure_list(h))) return r;
+    unsigned long long *d = reinterpret_cast<unsigned long long *>(h->d_sums);
+    CUDA_TRY(h, cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), h->stream));
+    k_count_pairs<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n, d);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemcpyAsync(c, d, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  }
+  if (within_cutoff) *within_cutoff = (int64_t)c[0];
+  if (list_entries) *list_entries = (int64_t)c[1];
   return MDG_OK;
 }
 

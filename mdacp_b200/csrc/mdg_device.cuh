@@ -56,8 +56,8 @@ struct Status {
   unsigned long long vmax2_bits;    // max |v|^2 of the last velocity update (double bits)
   double budget;                    // PairList::buffer_length
   unsigned long long dr2max_bits;   // displacement check: max |dq|^2
-  int cand_weighted;                // candidates counted with their image multiplicity
-  int cand_n;                       // candidate atoms stored
+  int cand_weighted;                // candidate copies (real atoms and ghost images)
+  int cand_n;                       // candidate copies stored
   int max_row;                      // longest neighbour row of the last build
   int want_build;                   // this step rebuilds the list
   long long list_entries;
@@ -82,8 +82,8 @@ struct Arrays {
   int *perm, *perm2;  // new slot -> old slot
   double4 *q_tmp, *v_tmp;
   int *ids_tmp, *type_tmp, *cell_tmp;
-  unsigned char *mult; // image multiplicity at the last build (1..27)
-  int *cand;          // displacement-check candidates
+  unsigned char *mult; // ghost-border membership at the last build (bits, see border_bits)
+  int2 *cand;         // displacement-check candidates: (slot, image code)
   double *partials;   // per-block partial sums for reductions
   Status *st;
   int stride;         // column stride of nbr (>= cap, multiple of 32)
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(BLOCK) k_vmax(Arrays a, int n) {
 // while the budget is positive (a too-fast atom is an error), then arm the
 // displacement check once the budget is spent.  Sets the two conditional
 // handles of this step's graph (or a device flag in eager mode).
-__global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_disp, int in_graph,
+static __global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_disp, int in_graph,
                          int *eager_flags) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   Status *st = a.st;
@@ -228,66 +228,124 @@ __global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_disp, int
 
 // Sets the rebuild condition of this step from the expiry and displacement
 // decisions.
-__global__ void k_decide(Arrays a, cudaGraphConditionalHandle h_build, int in_graph, int *eager_flags) {
+static __global__ void k_decide(Arrays a, cudaGraphConditionalHandle h_build, int in_graph, int *eager_flags) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int build = (a.st->error == 0) && a.st->want_build;
   if (in_graph) cudaGraphSetConditional(h_build, build);
   else eager_flags[1] = build;
 }
 
-// PairList::CheckByDisplacement, first pass: max |q_old - q|^2 (src/pairlist.cc:67-84).
+// ---- ghost copies of the reference, for the skin check -----------------
+// The reference checks displacements over real atoms AND their ghost
+// copies (src/pairlist.cc:67-121 loops over GetTotalParticleNumber()).  A
+// ghost is q + diff with diff = +L for atoms in a low-face strip and -L for a
+// high-face strip, per axis, for every combination of the strips the atom was
+// in at the last build (the six sequential border passes,
+// src/mdmanager.cc:395-401).  Its old position is the build-time copy; its
+// current one dates from the last SendBorderParticles, i.e. half a step back
+// after a full NVE / Nose-Hoover step (lag = dt/2; 0 otherwise).  An image
+// code holds 2 bits per axis: 0 no shift, 1 +L, 2 -L; code 0 is the atom.
+__device__ __forceinline__ double image_coord(double x, int c, double L) {
+  return c == 1 ? dadd(x, L) : (c == 2 ? dadd(x, -L) : x);
+}
+
+// The axis options of an atom's copies: mask bits 2d (low strip) and 2d+1
+// (high strip) for axis d.
+__device__ __forceinline__ int axis_options(int mask, int d, int opt[2]) {
+  int k = 0;
+  if (mask & (1 << (2 * d))) opt[k++] = 1;
+  if (mask & (1 << (2 * d + 1))) opt[k++] = 2;
+  return k;
+}
+
+// The state arrays the copy helpers read.
+struct CopyView {
+  const double4 *q_old, *q, *v;
+  const unsigned char *mask;
+};
+
+// Old and current position of copy `code` of atom i in a box of lengths L.
+__device__ __forceinline__ void copy_positions(const CopyView &cv, const double L[3], int i, int code, double lag,
+                                               double old_p[3], double new_p[3]) {
+  const double4 o = cv.q_old[i], q = cv.q[i];
+  const double oo[3] = {o.x, o.y, o.z};
+  double qq[3] = {q.x, q.y, q.z};
+  if (code != 0 && lag > 0.0) {
+    const double4 v = cv.v[i];
+    qq[0] = dsub(q.x, dmul(v.x, lag));
+    qq[1] = dsub(q.y, dmul(v.y, lag));
+    qq[2] = dsub(q.z, dmul(v.z, lag));
+  }
+  for (int d = 0; d < 3; d++) {
+    const int c = (code >> (2 * d)) & 3;
+    old_p[d] = image_coord(oo[d], c, L[d]);
+    new_p[d] = image_coord(qq[d], c, L[d]);
+  }
+}
+
+__device__ __forceinline__ double dist2(const double a[3], const double c[3]) {
+  const double dx = dsub(a[0], c[0]), dy = dsub(a[1], c[1]), dz = dsub(a[2], c[2]);
+  return dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+}
+
+// Calls f(code, d2) for every copy of atom i (the atom first), d2 the
+// squared displacement since the last build as the reference forms it
+// (qb_old - q, src/pairlist.cc:75-79).
+template <typename F>
+__device__ __forceinline__ void for_each_copy(const CopyView &cv, const double L[3], int i, double lag, F f) {
+  const int mask = cv.mask[i];
+  int ox[3] = {0, 0, 0}, oy[3] = {0, 0, 0}, oz[3] = {0, 0, 0};
+  int tx[2], ty[2], tz[2];
+  const int nx = axis_options(mask, 0, tx), ny = axis_options(mask, 1, ty), nz = axis_options(mask, 2, tz);
+  for (int k = 0; k < nx; k++) ox[k + 1] = tx[k];
+  for (int k = 0; k < ny; k++) oy[k + 1] = ty[k];
+  for (int k = 0; k < nz; k++) oz[k + 1] = tz[k];
+  for (int z = 0; z <= nz; z++)
+    for (int y = 0; y <= ny; y++)
+      for (int x = 0; x <= nx; x++) {
+        const int code = ox[x] | (oy[y] << 2) | (oz[z] << 4);
+        double op[3], np[3];
+        copy_positions(cv, L, i, code, lag, op, np);
+        f(code, dist2(op, np));
+      }
+}
+
+__device__ __forceinline__ CopyView copy_view(const Arrays &a) { return CopyView{a.q_old, a.q, a.v, a.mult}; }
+
+// PairList::CheckByDisplacement, first pass: max |qb_old - q|^2 over all
+// copies (src/pairlist.cc:67-84).
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_disp_max(Arrays a, int n) {
+__global__ void __launch_bounds__(BLOCK) k_disp_max(Arrays a, Box b, int n, double lag) {
   const int i = blockIdx.x * BLOCK + threadIdx.x;
   double d2 = 0.0;
-  if (i < n) {
-    const double4 q = a.q[i], o = a.q_old[i];
-    const double dx = dsub(o.x, q.x), dy = dsub(o.y, q.y), dz = dsub(o.z, q.z);
-    d2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-  }
+  if (i < n) for_each_copy(copy_view(a), b.L, i, lag, [&](int, double x) { d2 = fmax(d2, x); });
   block_max_to<BLOCK>(&a.st->dr2max_bits, d2);
 }
 
-// Second pass: atoms that moved more than BufferLength - sqrt(dr2_max)
-// (src/pairlist.cc:86-97).  Each real atom stands for its ghost images too,
-// so it is counted with its image multiplicity, as the reference's loop over
-// real + ghost atoms counts it.
+// Second pass: copies that moved more than BufferLength - sqrt(dr2_max)
+// (src/pairlist.cc:86-97); each is stored as (slot, image code).
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_disp_collect(Arrays a, Box b, int n, int cand_cap) {
+__global__ void __launch_bounds__(BLOCK) k_disp_collect(Arrays a, Box b, int n, int cand_cap, double lag) {
   const int i = blockIdx.x * BLOCK + threadIdx.x;
-  bool is_cand = false;
-  int m = 0;
-  if (i < n) {
-    const double dr2_max = __longlong_as_double((long long)a.st->dr2max_bits);
-    const double c = b.buffer_length - sqrt(dr2_max);
-    const double c_d2 = c * c;
-    const double4 q = a.q[i], o = a.q_old[i];
-    const double dx = dsub(o.x, q.x), dy = dsub(o.y, q.y), dz = dsub(o.z, q.z);
-    const double d2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-    is_cand = d2 > c_d2;
-    m = is_cand ? (int)a.mult[i] : 0;
-  }
-  const unsigned ball = __ballot_sync(0xffffffffu, is_cand);
-  const int wsum = __reduce_add_sync(0xffffffffu, m);
-  const int lane = threadIdx.x & 31;
-  int base = 0;
-  if (lane == 0 && ball) {
-    base = atomicAdd(&a.st->cand_n, __popc(ball));
-    atomicAdd(&a.st->cand_weighted, wsum);
-  }
-  base = __shfl_sync(0xffffffffu, base, 0);
-  if (is_cand) {
-    const int k = base + __popc(ball & ((1u << lane) - 1u));
-    if (k < cand_cap) a.cand[k] = i;
-  }
+  if (i >= n) return;
+  const double c = b.buffer_length - sqrt(__longlong_as_double((long long)a.st->dr2max_bits));
+  const double c_d2 = c * c;
+  for_each_copy(copy_view(a), b.L, i, lag, [&](int code, double d2) {
+    if (d2 > c_d2) {
+      atomicAdd(&a.st->cand_weighted, 1);
+      const int k = atomicAdd(&a.st->cand_n, 1);
+      if (k < cand_cap) a.cand[k] = make_int2(i, code);
+    }
+  });
 }
 
-// Third pass, one block: expired if the candidate count reaches
-// min(total atoms incl. images, CheckListLength), or if a candidate pair that
+// Third pass, one block: expired if the copies found reach
+// min(total copies, CheckListLength), or if a pair of candidate copies that
 // was at least SearchLength apart at the last build is now inside the
-// cut-off (src/pairlist.cc:86-121).  Minimum image replaces the ghost copies.
+// cut-off (src/pairlist.cc:86-121).  Copies carry their shifts, so the
+// distances are the reference's direct differences.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_disp_pairs(Arrays a, Box b) {
+__global__ void __launch_bounds__(BLOCK) k_disp_pairs(Arrays a, Box b, double lag) {
   __shared__ volatile int found;
   if (threadIdx.x == 0) found = 0;
   __syncthreads();
@@ -298,28 +356,17 @@ __global__ void __launch_bounds__(BLOCK) k_disp_pairs(Arrays a, Box b) {
     if (threadIdx.x == 0) found = 1;
   } else {
     const int l = min(st->cand_n, b.check_list_length);
-    const long long npairs = (long long)l * (l - 1) / 2;
-    for (long long p = threadIdx.x; p < npairs && !found; p += BLOCK) {
-      // unrank p -> (r, c) with r < c
-      long long r = (long long)((2.0 * l - 1.0 - sqrt((2.0 * l - 1.0) * (2.0 * l - 1.0) - 8.0 * p)) * 0.5);
-      if (r < 0) r = 0;
-      while (r > 0 && r * (2LL * l - r - 1) / 2 > p) r--;
-      while ((r + 1) * (2LL * l - r - 2) / 2 <= p) r++;
-      const long long c = p - r * (2LL * l - r - 1) / 2 + r + 1;
-      if (r >= l || c >= l || c <= r) continue;
-      const int i1 = a.cand[r], i2 = a.cand[c];
-      const double4 o1 = a.q_old[i1], o2 = a.q_old[i2];
-      double dx = o1.x - image_of(o2.x, o1.x, b.L[0], b.hL[0]);
-      double dy = o1.y - image_of(o2.y, o1.y, b.L[1], b.hL[1]);
-      double dz = o1.z - image_of(o2.z, o1.z, b.L[2], b.hL[2]);
-      double dr2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-      if (dr2 < b.sl2) continue;
-      const double4 n1 = a.q[i1], n2 = a.q[i2];
-      dx = n1.x - image_of(n2.x, n1.x, b.L[0], b.hL[0]);
-      dy = n1.y - image_of(n2.y, n1.y, b.L[1], b.hL[1]);
-      dz = n1.z - image_of(n2.z, n1.z, b.L[2], b.hL[2]);
-      dr2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-      if (dr2 < b.rc2) found = 1;
+    for (int r = 0; r < l - 1 && !found; r++) {
+      const int2 e1 = a.cand[r];
+      double o1[3], n1[3];
+      copy_positions(copy_view(a), b.L, e1.x, e1.y, lag, o1, n1);
+      for (int c = r + 1 + threadIdx.x; c < l; c += BLOCK) {
+        const int2 e2 = a.cand[c];
+        double o2[3], n2[3];
+        copy_positions(copy_view(a), b.L, e2.x, e2.y, lag, o2, n2);
+        if (dist2(o1, o2) < b.sl2) continue;
+        if (dist2(n1, n2) < b.rc2) found = 1;
+      }
     }
   }
   __syncthreads();
@@ -393,7 +440,7 @@ __global__ void __launch_bounds__(BLOCK) k_scatter(Arrays a, int n) {
 
 // Rebuild 4/6: order every cell by upload id (one warp per cell), which makes
 // the slot order a function of the state alone, independent of atomics.
-__global__ void k_sort_cells(Arrays a, int ncell) {
+static __global__ void k_sort_cells(Arrays a, int ncell) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= ncell || a.st->error) return;
@@ -419,22 +466,25 @@ __global__ void k_sort_cells(Arrays a, int ncell) {
   }
 }
 
-// Image multiplicity of a wrapped position: the number of ghost copies the
-// reference's six sequential border passes make of it, times itself
-// (src/mdmanager.cc:395-401, MDRect::IsInsideEdge src/mdrect.cc:23-47).
-__device__ __forceinline__ int image_multiplicity(const double x[3], const Box &b) {
-  int m = 1;
+// Ghost-strip membership of a wrapped position at a build: bit 2d for
+// 0 < x_d < SL, bit 2d+1 for L_d - SL < x_d < L_d (MDRect::IsInsideEdge,
+// src/mdrect.cc:23-47); the copies are every combination of the strips, so
+// their count including the atom is the product over axes of (1 + bits).
+__device__ __forceinline__ int border_bits(const double x[3], const Box &b, int *copies) {
+  int mask = 0, m = 1;
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    const int k = 1 + ((x[d] < b.sl && x[d] > 0.0) ? 1 : 0) +
-                  ((x[d] > b.L[d] - b.sl && x[d] < b.L[d]) ? 1 : 0);
-    m *= k;
+    const int lo = (x[d] < b.sl && x[d] > 0.0) ? 1 : 0;
+    const int hi = (x[d] > b.L[d] - b.sl && x[d] < b.L[d]) ? 1 : 0;
+    mask |= (lo << (2 * d)) | (hi << (2 * d + 1));
+    m *= 1 + lo + hi;
   }
-  return m;
+  *copies = m;
+  return mask;
 }
 
 // Rebuild 5/6: gather into cell order (temporary arrays), snapshot q_old
-// (PairList::Init), image multiplicity.
+// (PairList::Init), ghost-strip membership and the total copy count.
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_permute(Arrays a, Box b, int n) {
   const int s = blockIdx.x * BLOCK + threadIdx.x;
@@ -449,8 +499,7 @@ __global__ void __launch_bounds__(BLOCK) k_permute(Arrays a, Box b, int n) {
     a.cell_tmp[s] = a.cell[o];
     a.q_old[s] = q;
     const double x[3] = {q.x, q.y, q.z};
-    m = image_multiplicity(x, b);
-    a.mult[s] = (unsigned char)m;
+    a.mult[s] = (unsigned char)border_bits(x, b, &m);
     // cell-local FP32 coordinates for the list prefilter
     const int c = a.cell_tmp[s];
     const int cx = c % b.ms[0], cy = (c / b.ms[0]) % b.ms[1], cz = c / (b.ms[0] * b.ms[1]);
@@ -537,7 +586,7 @@ __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
 }
 
 // Before a build: clear the build counters.
-__global__ void k_build_begin(Arrays a) {
+static __global__ void k_build_begin(Arrays a) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   a.st->max_row = 0;
   a.st->list_entries = 0;
@@ -546,7 +595,7 @@ __global__ void k_build_begin(Arrays a) {
 
 // After a build: fresh skin budget (PairList::Init, src/pairlist.cc:10-23),
 // counters, |v|^2 max for the next expiry test is untouched.
-__global__ void k_build_done(Arrays a, Box b) {
+static __global__ void k_build_done(Arrays a, Box b) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   Status *st = a.st;
   if (st->error) return;
@@ -899,8 +948,35 @@ __global__ void __launch_bounds__(BLOCK) k_final_sum(const double *partials, int
     for (int k = 0; k < NSUM; k++) out[k] = sm[k][0];
 }
 
+// Directed list entries within the cut-off (the pairs whose force is
+// evaluated), with the reference's r^2 test (src/fcalculator.cc:268), summed
+// into counts[0]; counts[1] gets all list entries.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_count_pairs(Arrays a, Box b, int n, unsigned long long *counts) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  int within = 0, nn = 0;
+  if (i < n) {
+    const double4 qi = a.q[i];
+    nn = a.nnbr[i];
+    for (int k = 0; k < nn; k++) {
+      const double4 qj = a.q[a.nbr[(size_t)k * a.stride + i]];
+      const double dx = dsub(image_of(qj.x, qi.x, b.L[0], b.hL[0]), qi.x);
+      const double dy = dsub(image_of(qj.y, qi.y, b.L[1], b.hL[1]), qi.y);
+      const double dz = dsub(image_of(qj.z, qi.z, b.L[2], b.hL[2]), qi.z);
+      const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+      within += (r2 > b.rc2) ? 0 : 1;
+    }
+  }
+  const int ws = __reduce_add_sync(0xffffffffu, within);
+  const int ns = __reduce_add_sync(0xffffffffu, nn);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&counts[0], (unsigned long long)ws);
+    atomicAdd(&counts[1], (unsigned long long)ns);
+  }
+}
+
 // End of step bookkeeping (MDManager::Calculate: s_time += TimeStep).
-__global__ void k_step_done(Arrays a, Box b) {
+static __global__ void k_step_done(Arrays a, Box b) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   if (a.st->error) return;
   a.st->steps++;

@@ -32,6 +32,7 @@ __all__ = [
     "config_c1",
     "config_c2",
     "config_c3",
+    "config_c4",
     "config_c5",
 ]
 
@@ -106,90 +107,48 @@ def fcc_liquid(ncells, rho: float, temperature: float, seed: int, jitter: float 
                  dt=dt, temperature=temperature, name=name)
 
 
-def _rsa_fill(rng, lo, hi, count, r_min, existing=None, batch=None):
-    """Random sequential addition of ``count`` points uniformly in the box
-    ``[lo, hi)`` with no two points (including ``existing``) closer than
-    ``r_min``.  Candidates are tested in batches against a cell grid."""
-    lo = np.asarray(lo, dtype=np.float64)
-    hi = np.asarray(hi, dtype=np.float64)
-    width = hi - lo
-    ncell = np.maximum(1, np.floor(width / r_min).astype(np.int64))
-    csize = width / ncell
-    slots = 8
-    grid = np.full((ncell[0], ncell[1], ncell[2], slots), -1, dtype=np.int64)
-    fill = np.zeros((ncell[0], ncell[1], ncell[2]), dtype=np.int64)
-    pts = np.empty((count, 3), dtype=np.float64)
-    n = 0
-    r2 = r_min * r_min
-    offs = np.array([[dx, dy, dz] for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)])
+_rsa_lib = None
 
-    def cell_of(p):
-        c = np.floor((p - lo) / csize).astype(np.int64)
-        return np.minimum(np.maximum(c, 0), ncell - 1)
 
-    all_pts = [] if existing is None else [existing]
-    base = 0 if existing is None else existing.shape[0]
-    store = np.empty((base + count, 3), dtype=np.float64)
-    if existing is not None:
-        store[:base] = existing
-        c = cell_of(existing)
-        for k in range(base):  # existing points are few (vapour next to liquid only)
-            cx, cy, cz = c[k]
-            grid[cx, cy, cz, fill[cx, cy, cz]] = k
-            fill[cx, cy, cz] += 1
-    total = base
-    batch = batch or max(1024, count // 4)
-    while n < count:
-        m = min(batch, 2 * (count - n) + 256)
-        cand = lo + rng.random((m, 3)) * width
-        cc = cell_of(cand)
-        # conflicts with accepted points
-        nb = cc[:, None, :] + offs[None, :, :]
-        ok = np.ones(m, dtype=bool)
-        for d in range(3):  # periodic only along axes that span the whole box
-            nb[..., d] = np.mod(nb[..., d], ncell[d])
-        ids = grid[nb[..., 0], nb[..., 1], nb[..., 2]]  # (m, 27, slots)
-        valid = ids >= 0
-        other = store[np.where(valid, ids, 0)]
-        diff = other - cand[:, None, None, :]
-        diff -= width * np.round(diff / width)
-        close = (np.einsum("mksd,mksd->mks", diff, diff) < r2) & valid
-        ok &= ~close.any(axis=(1, 2))
-        # conflicts inside the batch: keep a candidate only if no earlier
-        # accepted-so-far candidate of this batch is within r_min
-        idx = np.nonzero(ok)[0]
-        keep = []
-        bgrid = {}
-        for k in idx:
-            cx, cy, cz = cc[k]
-            clash = False
-            for o in offs:
-                key = ((cx + o[0]) % ncell[0], (cy + o[1]) % ncell[1], (cz + o[2]) % ncell[2])
-                for j in bgrid.get(key, ()):
-                    dd = cand[j] - cand[k]
-                    dd -= width * np.round(dd / width)
-                    if dd @ dd < r2:
-                        clash = True
-                        break
-                if clash:
-                    break
-            if clash:
-                continue
-            if fill[cx, cy, cz] >= slots:
-                continue
-            bgrid.setdefault((cx, cy, cz), []).append(k)
-            keep.append(k)
-            if n + len(keep) >= count:
-                break
-        for k in keep:
-            cx, cy, cz = cc[k]
-            store[total] = cand[k]
-            grid[cx, cy, cz, fill[cx, cy, cz]] = total
-            fill[cx, cy, cz] += 1
-            total += 1
-        pts[n:n + len(keep)] = cand[keep]
-        n += len(keep)
-    return pts
+def _rsa():
+    """ctypes handle of libmdg_workloads.so (built next to libmdacp_b200.so)."""
+    global _rsa_lib
+    if _rsa_lib is None:
+        import ctypes
+        import pathlib
+
+        path = pathlib.Path(__file__).resolve().parent / "libmdg_workloads.so"
+        if not path.exists():
+            raise FileNotFoundError(f"{path} is not built (make -C mdacp_b200/csrc)")
+        lib = ctypes.CDLL(str(path))
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.mdg_rsa_fill.restype = ctypes.c_long
+        lib.mdg_rsa_fill.argtypes = [dp, ctypes.c_double, ctypes.c_int, dp, dp,
+                                     ctypes.POINTER(ctypes.c_long), ctypes.c_uint64, ctypes.c_long, dp]
+        _rsa_lib = lib
+    return _rsa_lib
+
+
+def rsa_fill(L, r_min, regions, counts, seed, max_tries=None):
+    """Random sequential addition: counts[k] points uniform in region k
+    (lo, hi corners), all at periodic distance >= r_min in the box L."""
+    import ctypes
+
+    lib = _rsa()
+    L = np.ascontiguousarray(L, dtype=np.float64)
+    lo = np.ascontiguousarray([r[0] for r in regions], dtype=np.float64)
+    hi = np.ascontiguousarray([r[1] for r in regions], dtype=np.float64)
+    cnt = np.ascontiguousarray(counts, dtype=np.int64)
+    total = int(cnt.sum())
+    out = np.zeros((max(total, 1), 3), dtype=np.float64)
+    dp = ctypes.POINTER(ctypes.c_double)
+    got = lib.mdg_rsa_fill(L.ctypes.data_as(dp), float(r_min), len(regions), lo.ctypes.data_as(dp),
+                           hi.ctypes.data_as(dp), cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_long)),
+                           int(seed) & 0xFFFFFFFFFFFFFFFF, int(max_tries or 200 * total + 1000),
+                           out.ctypes.data_as(dp))
+    if got != total:
+        raise RuntimeError(f"random sequential addition placed {got} of {total} points")
+    return out[:total]
 
 
 def slab(n_total: int, rho_liquid: float, rho_vapour: float, temperature: float, seed: int,
@@ -197,8 +156,9 @@ def slab(n_total: int, rho_liquid: float, rho_vapour: float, temperature: float,
          name: str = "") -> State:
     """Liquid slab (density ``rho_liquid``) filling the middle ``1/aspect`` of
     the long z axis of an ``1:1:aspect`` box, vapour (``rho_vapour``)
-    elsewhere; uniform random positions with overlap rejection at ``r_min``.
-    The box volume is chosen so that the expected atom count is ``n_total``."""
+    elsewhere; uniform random positions with overlaps below ``r_min``
+    rejected (random sequential addition over the whole periodic box).  The
+    box volume is chosen so that the expected atom count is ``n_total``."""
     frac = 1.0 / aspect
     mean_rho = frac * rho_liquid + (1.0 - frac) * rho_vapour
     vol = n_total / mean_rho
@@ -208,60 +168,13 @@ def slab(n_total: int, rho_liquid: float, rho_vapour: float, temperature: float,
     z1 = z0 + frac * L[2]
     n_liq = int(round(rho_liquid * lx * lx * (z1 - z0)))
     n_vap = n_total - n_liq
+    n_low = n_vap // 2
+    regions = [([0.0, 0.0, z0], [lx, lx, z1]), ([0.0, 0.0, 0.0], [lx, lx, z0]), ([0.0, 0.0, z1], [lx, lx, L[2]])]
+    q = rsa_fill(L, r_min, regions, [n_liq, n_low, n_vap - n_low], seed)
     rng = np.random.Generator(np.random.Philox(seed))
-    liq = _rsa_fill(rng, [0.0, 0.0, z0], [lx, lx, z1], n_liq, r_min)
-    # vapour: uniform in the two outer regions, away from the slab by r_min
-    vap = []
-    need = n_vap
-    while need > 0:
-        m = 2 * need + 64
-        cand = rng.random((m, 3)) * L
-        outside = (cand[:, 2] < z0 - r_min) | (cand[:, 2] > z1 + r_min)
-        cand = cand[outside]
-        vap.append(cand)
-        need -= cand.shape[0]
-    vap = np.concatenate(vap)[:n_vap]
-    vap = _dedupe_vapour(vap, L, r_min)
-    q = np.concatenate([liq, vap])
     v = maxwell_boltzmann(q.shape[0], temperature, rng)
     ids = np.arange(q.shape[0], dtype=np.int32)
     return State(q=q, v=v, ids=ids, L=L, rc=rc, dt=dt, temperature=temperature, name=name)
-
-
-def _dedupe_vapour(p, L, r_min):
-    """Drops vapour points that overlap an earlier one (vapour is dilute, so
-    this removes a handful at most)."""
-    keep = np.ones(p.shape[0], dtype=bool)
-    cell = np.floor(p / r_min).astype(np.int64)
-    ncell = np.maximum(1, np.floor(L / r_min).astype(np.int64))
-    cell = np.minimum(cell, ncell - 1)
-    key = (cell[:, 0] * ncell[1] + cell[:, 1]) * ncell[2] + cell[:, 2]
-    order = np.argsort(key, kind="stable")
-    seen = {}
-    for k in order:
-        cx, cy, cz = cell[k]
-        clash = False
-        for dx in (-1, 0, 1):
-            for dy in (-1, 0, 1):
-                for dz in (-1, 0, 1):
-                    kk = ((cx + dx) % ncell[0], (cy + dy) % ncell[1], (cz + dz) % ncell[2])
-                    for j in seen.get(kk, ()):
-                        d = p[j] - p[k]
-                        d -= L * np.round(d / L)
-                        if d @ d < r_min * r_min:
-                            clash = True
-                            break
-                    if clash:
-                        break
-                if clash:
-                    break
-            if clash:
-                break
-        if clash:
-            keep[k] = False
-        else:
-            seen.setdefault((cx, cy, cz), []).append(k)
-    return p[keep]
 
 
 def config_c1(seed: int = 12345) -> State:
@@ -286,3 +199,24 @@ def config_c3(seed: int = 31, n_total: int = 1_000_000) -> State:
 def config_c5(seed: int = 55) -> State:
     """32,000 atoms, FCC 20^3 cells, rho = 0.8442, T = 1.0, rc = 2.5, dt = 0.005."""
     return fcc_liquid(20, 0.8442, 1.0, seed, rc=2.5, dt=0.005, name="lj_fcc32000_rho0.8442")
+
+
+def config_c4(seed: int = 404, nrep: int = 256, n_range=(500, 20000), rho_range=(0.3, 0.9),
+              t_range=(0.7, 1.5), jitter: float = 0.05):
+    """Replica ensemble: ``nrep`` jittered FCC systems, N uniform in
+    ``n_range`` (rounded to an FCC block of nx x nx x nz cells), density and
+    temperature uniform in their ranges, all drawn from one seed; rc = 2.5,
+    dt = 0.005."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for k in range(nrep):
+        n_target = rng.uniform(*n_range)
+        rho = rng.uniform(*rho_range)
+        temp = rng.uniform(*t_range)
+        nx = max(1, int(round((n_target / 4.0) ** (1.0 / 3.0))))
+        nz = max(1, int(round(n_target / (4.0 * nx * nx))))
+        rep_seed = int(rng.integers(0, 2**31))
+        st = fcc_liquid((nx, nx, nz), rho, temp, rep_seed, jitter=jitter, rc=2.5, dt=0.005,
+                        name=f"replica{k}")
+        out.append(st)
+    return out
