@@ -126,6 +126,18 @@ __device__ __forceinline__ void block_max_to(unsigned long long *addr, double v)
   }
 }
 
+// Warp maximum folded into a global maximum without a block barrier, so a
+// warp that finishes its rows early leaves at once; the atomic is skipped
+// when the global value is already at least as large (non-negative v).
+__device__ __forceinline__ void warp_max_to(unsigned long long *addr, double v) {
+  v = warp_max(v);
+  if ((threadIdx.x & 31) == 0 && v > 0.0) {
+    const unsigned long long cur = *(volatile unsigned long long *)addr;
+    const unsigned long long mine = (unsigned long long)__double_as_longlong(v);
+    if (mine > cur) atomicMax(addr, mine);
+  }
+}
+
 // Fixed order block sum written to partials[blockIdx.x * nsum + k].
 template <int BLOCK, int NSUM>
 __device__ __forceinline__ void block_sum_to(double (&v)[NSUM], double *partials) {
@@ -510,6 +522,17 @@ __global__ void __launch_bounds__(BLOCK) k_permute(Arrays a, Box b, int n) {
   if ((threadIdx.x & 31) == 0 && tot) atomicAdd((unsigned long long *)&a.st->total_images, (unsigned long long)tot);
 }
 
+// Strip bits a partner needs for its ghost copy with shift (sx, sy, sz) to
+// exist: +L images come from the low-face strip, -L images from the high-face
+// strip (MDUnit::MakeBufferForBorderParticles, src/mdunit.cc:156-192).  A
+// partner outside the strip -- e.g. exactly on a face, which the strict
+// MDRect::IsInsideEdge test leaves out (src/mdrect.cc:27-43) -- has no copy
+// there, and the reference's search does not see that pair from this side.
+__device__ __forceinline__ int needed_strips(double sx, double sy, double sz) {
+  return (sx > 0.0 ? 1 : 0) | (sx < 0.0 ? 2 : 0) | (sy > 0.0 ? 4 : 0) | (sy < 0.0 ? 8 : 0) |
+         (sz > 0.0 ? 16 : 0) | (sz < 0.0 ? 32 : 0);
+}
+
 // Exact test of one candidate, the reference's arithmetic
 // (MeshList::SearchMesh, src/meshlist.cc:276-289): ghost image q_j + diff
 // first, then dx = x_i - image, then ((dx*dx + dy*dy) + dz*dz), each
@@ -558,11 +581,13 @@ __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
           const float bx = (float)((x - cx) * b.cs[0] + sx) - li.x;
           const int nc = (z * b.ms[1] + y) * b.ms[0] + x;
           const int beg = a.cell_start[nc], end = a.cell_start[nc + 1];
+          const int need = needed_strips(sx, sy, sz);
           for (int j = beg; j < end; j++) {
             const float4 lj = a.qloc[j];
             const float ex = lj.x + bx, ey = lj.y + by, ez = lj.z + bz;
             const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
             if (r2 > hi || j == i) continue;
+            if (need && (a.mult[j] & need) != need) continue;
             if (r2 >= lo && !within_search_exact(a.q[i], a.q[j], sx, sy, sz, b.sl2)) continue;
             if (cnt < maxnb) a.nbr[(size_t)cnt * stride + i] = j;
             cnt++;
@@ -740,7 +765,7 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp64(Arrays a, Box b, int n, Th
     }
     finish_atom<MODE>(a, b, th, i, fx, fy, fz, v2, ke);
   }
-  if (MODE == kKickLangevin) block_max_to<BLOCK>(&a.st->vmax2_bits, v2);
+  if (MODE == kKickLangevin) warp_max_to(&a.st->vmax2_bits, v2);
   if (MODE == kKickNoseHoover) {
     double s[1] = {ke};
     block_sum_to<BLOCK, 1>(s, a.partials);
@@ -778,7 +803,8 @@ __device__ __forceinline__ void lj_pair_fp32(const int4 &pi, const int4 &pj, flo
 // FP32-mixed force kick.  Displacements come from the fixed-point copy (no
 // ghost atoms, no shift codes).  Rows are padded to a multiple of 4, so the
 // row is walked four partners at a time without per-lane masks, with the
-// next four indices loaded ahead; FP32 partial sums over 8 partners are
+// indices of the next eight partners already in flight (the list is the one
+// stream from HBM, so its loads are issued two groups ahead); FP32 partial sums over 8 partners are
 // folded into an FP64 per-atom sum; the kick is FP64.  With DRIFT the second
 // half drift q += v dt/2 and the |v| maximum of the step are done in the
 // same pass: this kernel reads only the fixed-point copy, so moving q here
@@ -798,23 +824,34 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Th
     double Fx = 0.0, Fy = 0.0, Fz = 0.0;
     float fx = 0.f, fy = 0.f, fz = 0.f;
     int n0 = i, n1 = i, n2 = i, n3 = i;
+    int m0 = i, m1 = i, m2 = i, m3 = i;
     if (nn4 > 0) {
       n0 = __ldg(row);
       n1 = __ldg(row + st);
       n2 = __ldg(row + 2 * st);
       n3 = __ldg(row + 3 * st);
     }
+    if (nn4 > 4) {
+      m0 = __ldg(row + 4 * st);
+      m1 = __ldg(row + 5 * st);
+      m2 = __ldg(row + 6 * st);
+      m3 = __ldg(row + 7 * st);
+    }
     for (int k = 0; k < nn4; k += 4) {
       const int4 p0 = __ldg(a.qfix + n0);
       const int4 p1 = __ldg(a.qfix + n1);
       const int4 p2 = __ldg(a.qfix + n2);
       const int4 p3 = __ldg(a.qfix + n3);
-      if (k + 4 < nn4) {
-        const int *r = row + (size_t)(k + 4) * st;
-        n0 = __ldg(r);
-        n1 = __ldg(r + st);
-        n2 = __ldg(r + 2 * st);
-        n3 = __ldg(r + 3 * st);
+      n0 = m0;
+      n1 = m1;
+      n2 = m2;
+      n3 = m3;
+      if (k + 8 < nn4) {
+        const int *r = row + (size_t)(k + 8) * st;
+        m0 = __ldg(r);
+        m1 = __ldg(r + st);
+        m2 = __ldg(r + 2 * st);
+        m3 = __ldg(r + 3 * st);
       }
       lj_pair_fp32(pi, p0, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
       lj_pair_fp32(pi, p1, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
@@ -844,7 +881,7 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Th
       if (!isfinite(v2) || !isfinite(q.x + q.y + q.z)) atomicOr(&a.st->error, kErrNonFinite);
     }
   }
-  if (MODE == kKickLangevin || DRIFT) block_max_to<BLOCK>(&a.st->vmax2_bits, v2);
+  if (MODE == kKickLangevin || DRIFT) warp_max_to(&a.st->vmax2_bits, v2);
   if (MODE == kKickNoseHoover) {
     double s[1] = {ke};
     block_sum_to<BLOCK, 1>(s, a.partials);

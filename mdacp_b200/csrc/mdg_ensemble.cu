@@ -404,6 +404,8 @@ __global__ void __launch_bounds__(kEF) ke_build(Ens e) {
       const double sx = tx > rep.hL[0] ? -rep.L[0] : (tx < -rep.hL[0] ? rep.L[0] : 0.0);
       const double sy = ty > rep.hL[1] ? -rep.L[1] : (ty < -rep.hL[1] ? rep.L[1] : 0.0);
       const double sz = tz > rep.hL[2] ? -rep.L[2] : (tz < -rep.hL[2] ? rep.L[2] : 0.0);
+      const int need = needed_strips(sx, sy, sz);
+      if (need && (e.mult[j] & need) != need) continue;
       if (!within_search_exact(qi, qj, sx, sy, sz, e.sl2)) continue;
       if (cnt < maxnb) e.nbr[(size_t)cnt * stride + i] = j;
       cnt++;
@@ -430,11 +432,13 @@ __global__ void __launch_bounds__(kEF) ke_build(Ens e) {
           const float bx = (float)((x - cx) * rep.cs[0] + sx) - li.x;
           const int nc = rep.cell_off + (z * rep.ms[1] + y) * rep.ms[0] + x;
           const int beg = e.cell_start[nc], end = e.cell_start[nc + 1];
+          const int need = needed_strips(sx, sy, sz);
           for (int j = beg; j < end; j++) {
             const float4 lj = e.qloc[j];
             const float ex = lj.x + bx, ey = lj.y + by, ez = lj.z + bz;
             const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
             if (r2 > hi || j == i) continue;
+            if (need && (e.mult[j] & need) != need) continue;
             if (r2 >= lo && !within_search_exact(e.q[i], e.q[j], sx, sy, sz, e.sl2)) continue;
             if (cnt < maxnb) e.nbr[(size_t)cnt * stride + i] = j;
             cnt++;
@@ -509,24 +513,36 @@ __global__ void __launch_bounds__(kEF) ke_force_fp32(Ens e) {
     const int st = e.stride;
     double Fx = 0.0, Fy = 0.0, Fz = 0.0;
     float fx = 0.f, fy = 0.f, fz = 0.f;
+    // indices of the next eight partners in flight, as in k_force_fp32
     int n0 = i, n1 = i, n2 = i, n3 = i;
+    int m0 = i, m1 = i, m2 = i, m3 = i;
     if (nn4 > 0) {
       n0 = __ldg(row);
       n1 = __ldg(row + st);
       n2 = __ldg(row + 2 * st);
       n3 = __ldg(row + 3 * st);
     }
+    if (nn4 > 4) {
+      m0 = __ldg(row + 4 * st);
+      m1 = __ldg(row + 5 * st);
+      m2 = __ldg(row + 6 * st);
+      m3 = __ldg(row + 7 * st);
+    }
     for (int k = 0; k < nn4; k += 4) {
       const int4 p0 = __ldg(e.qfix + n0);
       const int4 p1 = __ldg(e.qfix + n1);
       const int4 p2 = __ldg(e.qfix + n2);
       const int4 p3 = __ldg(e.qfix + n3);
-      if (k + 4 < nn4) {
-        const int *rr = row + (size_t)(k + 4) * st;
-        n0 = __ldg(rr);
-        n1 = __ldg(rr + st);
-        n2 = __ldg(rr + 2 * st);
-        n3 = __ldg(rr + 3 * st);
+      n0 = m0;
+      n1 = m1;
+      n2 = m2;
+      n3 = m3;
+      if (k + 8 < nn4) {
+        const int *rr = row + (size_t)(k + 8) * st;
+        m0 = __ldg(rr);
+        m1 = __ldg(rr + st);
+        m2 = __ldg(rr + 2 * st);
+        m3 = __ldg(rr + 3 * st);
       }
       lj_pair_fp32(pi, p0, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
       lj_pair_fp32(pi, p1, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
