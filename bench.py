@@ -199,6 +199,8 @@ def main():
                     help="restrict the timed runs (profiling); the JSON line needs both")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end run (profiling)")
     ap.add_argument("--no-force-error", action="store_true", help="skip the FP32-vs-FP64 force check")
+    ap.add_argument("--drift-steps", type=int, default=2000,
+                    help="NVE steps of the energy-drift comparison of the two paths (0: skip)")
     ap.add_argument("--eager", action="store_true",
                     help="launch every kernel from the host instead of CUDA graphs (for profilers)")
     ap.add_argument("--config", choices=["c2", "c1", "c3", "c4"], default="c2",
@@ -284,10 +286,14 @@ def main_reference(args, ws, rank, state, config):
 
 
 def force_kernel_bytes(n, list_entries, precision):
-    """Algorithmic bytes of one force-kick launch (neighbour gathers count as
-    cache-served): own position + row length + list + velocity read/write."""
-    own = 16 if precision == "fp32" else 32
-    return n * (own + 4 + 32 + 32) + 4 * list_entries
+    """Algorithmic bytes of one force launch (neighbour gathers count as
+    cache-served).  FP64 kick: own position + row length + list + velocity
+    read/write.  FP32-mixed NVE pass (both half drifts fused): own
+    fixed-point copy + row length + list + velocity and position read/write
+    + the next step's fixed-point copy."""
+    if precision == "fp32":
+        return n * (16 + 4 + 64 + 64 + 16) + 4 * list_entries
+    return n * (32 + 4 + 32 + 32) + 4 * list_entries
 
 
 def timed_run(sys_, args, dist, device, torch):
@@ -402,6 +408,29 @@ def main_mdg(args, ws, rank, local, state, config):
             "rms": float(np.sqrt((d ** 2).mean()) / np.sqrt((mag ** 2).mean())),
             "state": "after 50 FP64 steps from the start state"}
 
+    # NVE energy drift of both paths from the same state (total energy per atom
+    # observed every 100 MD steps)
+    drift = None
+    if config.get("thermostat", "NVE") == "NVE" and args.drift_steps > 0:
+        drift = {"md_steps": args.drift_steps, "observe_every": 100, "state": "the start state"}
+        for prec_name, prec in (("fp32", M.FP32_MIXED), ("fp64", M.FP64)):
+            sd = M.System(state.L, precision=prec, device=local, **system_kwargs(state, config, M))
+            sd.set_state(state.q, state.v)
+            ke, pe, _ = sd.observe()
+            e0 = (ke + pe) / n
+            es = [e0]
+            for _ in range(max(1, args.drift_steps // 100)):
+                sd.calculate(100)
+                ke, pe, _ = sd.observe()
+                es.append((ke + pe) / n)
+            sd.close()
+            es = np.asarray(es)
+            t = np.arange(len(es)) * 100 * state.dt
+            slope = float(np.polyfit(t, es, 1)[0]) if len(es) > 2 else 0.0
+            drift[prec_name] = {"e0_per_atom": float(e0), "max_abs_dev_per_atom": float(np.abs(es - e0).max()),
+                                "max_rel_dev": float(np.abs(es - e0).max() / abs(e0)),
+                                "slope_per_atom_per_time": slope}
+
     r32, r64 = result["fp32"], result["fp64"]
     hbm, peak_kind = peaks()
     rebuilds = r32["info1"]["rebuilds"] - r32["info0"]["rebuilds"]
@@ -428,8 +457,9 @@ def main_mdg(args, ws, rank, local, state, config):
             "fp64": ws * r64["pairs"] * args.steps * args.md_steps_per_step / (r64["ms"] * 1e-3),
             "pairs_within_cutoff_per_step": r32["pairs"]},
         "force_error_fp32_vs_fp64": errs,
+        "nve_energy_drift": drift,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": traffic, "kernel": "k_force_fp32 (kick)",
+                     "frac": achieved / hbm, "traffic": traffic, "kernel": "k_force_fp32 (fused NVE step: drift, kick, drift, pack)",
                      "algorithmic_bytes_per_launch": fbytes, "avg_launch_ms": f_avg_ms,
                      "launches": r32["force_launches"], "peak_kind": peak_kind},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 32 * n,

@@ -51,6 +51,9 @@ struct mdg_handle {
   int64_t force_launches = 0;
   int64_t kernel_launches = 0;
   int graph_kernel_count = 0;         // kernels per graph launch outside conditionals
+  // fused FP32 NVE step: which fixed-point buffer (0: qfix, 1: qfix2) holds
+  // every atom's position after the coming step's first half drift; -1: none
+  int fix_buf = -1;
   std::string err;
 };
 
@@ -75,7 +78,7 @@ cudaError_t dalloc(T **p, size_t count) {
 }
 
 void free_arrays(Arrays &a) {
-  void *ptrs[] = {a.q, a.v, a.q_old, a.qfix, a.qloc, a.ids, a.type, a.cell, a.nbr, a.nnbr, a.cell_count,
+  void *ptrs[] = {a.q, a.v, a.q_old, a.qfix, a.qfix2, a.qloc, a.ids, a.type, a.cell, a.nbr, a.nnbr, a.cell_count,
                   a.cell_start, a.slot, a.perm, a.perm2, a.q_tmp, a.v_tmp, a.ids_tmp, a.type_tmp,
                   a.cell_tmp, a.mult, a.cand, a.partials, a.st};
   for (void *p : ptrs)
@@ -170,7 +173,9 @@ double step_lag(const mdg_handle *h) {
 }
 
 // Pairlist rebuild (MDManager::MakePairList).
-void launch_build(mdg_handle *h, cudaStream_t s) {
+// pack: where to put the coming step's first-drift positions after the
+// rebuild (the fused FP32 NVE step), or nullptr.
+void launch_build(mdg_handle *h, cudaStream_t s, int4 *pack = nullptr) {
   const int n = h->n;
   Arrays &a = h->a;
   k_build_begin<<<1, 32, 0, s>>>(a);
@@ -186,20 +191,35 @@ void launch_build(mdg_handle *h, cudaStream_t s) {
   cudaMemcpyAsync(a.type, a.type_tmp, sizeof(int) * n, cudaMemcpyDeviceToDevice, s);
   k_build<kForceBlock><<<blocks_for(n, kForceBlock), kForceBlock, 0, s>>>(a, h->box, n);
   k_build_done<<<1, 32, 0, s>>>(a, h->box);
+  if (pack) k_pack_half<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, h->box, n, pack);
 }
 
-// drift: also apply the second half drift in the same pass (FP32-mixed only;
-// returns false when the caller still has to launch the drift).
+// The FP32-mixed NVE step runs as one force pass per step (both half
+// drifts fused, the next step's fixed-point copy packed into the other
+// buffer).
+bool fused_step(const mdg_handle *h) {
+  return h->prm.precision == MDG_FP32_MIXED && h->prm.thermostat == MDG_NVE;
+}
+
+int4 *fix_buffer(mdg_handle *h, int k) { return k ? h->a.qfix2 : h->a.qfix; }
+
+// drift: 1 also applies the second half drift in the same pass, 2 the whole
+// fused NVE step reading qf and packing into qf_next (FP32-mixed only);
+// returns false when the caller still has to launch the second drift.
 template <int MODE>
-bool launch_force_mode(mdg_handle *h, cudaStream_t s, const Thermo &th, bool drift = false) {
+bool launch_force_mode(mdg_handle *h, cudaStream_t s, const Thermo &th, int drift = 0, const int4 *qf = nullptr,
+                       int4 *qf_next = nullptr) {
   const int n = h->n;
   const int nb = blocks_for(n, kForceBlock);
+  if (!qf) qf = h->a.qfix;
   if (h->prm.precision == MDG_FP32_MIXED) {
-    if (drift)
-      k_force_fp32<kForceBlock, MODE, true><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th);
+    if (drift == 2)
+      k_force_fp32<kForceBlock, MODE, 2><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, qf_next);
+    else if (drift)
+      k_force_fp32<kForceBlock, MODE, 1><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, nullptr);
     else
-      k_force_fp32<kForceBlock, MODE, false><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th);
-    return drift;
+      k_force_fp32<kForceBlock, MODE, 0><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, nullptr);
+    return drift != 0;
   }
   k_force_fp64<kForceBlock, MODE><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th);
   return false;
@@ -223,26 +243,35 @@ void launch_drift(mdg_handle *h, cudaStream_t s, bool pack_fix, int track_vmax) 
 
 // Everything of MDManager::Calculate after the rebuild decision; returns the
 // number of kernels launched.  ev_start/ev_stop bracket the force kernel.
+// parity: the fixed-point buffer the fused NVE step reads (it writes the
+// other one).
 int launch_step_tail(mdg_handle *h, cudaStream_t s, cudaEvent_t ev_start, cudaEvent_t ev_stop,
-                     bool capture) {
+                     bool capture, int parity) {
   const bool fix = h->prm.precision == MDG_FP32_MIXED;
   const Thermo th = thermo_of(h);
   const int n = h->n;
   int launches = 0;
-  launch_drift(h, s, fix, 0);
-  launches++;
   auto rec = [&](cudaEvent_t e) {
     if (!e) return;
     if (capture) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
     else cudaEventRecord(e, s);
   };
+  if (fused_step(h)) {
+    rec(ev_start);
+    launch_force_mode<kKick>(h, s, th, 2, fix_buffer(h, parity), fix_buffer(h, 1 - parity));
+    rec(ev_stop);
+    k_step_done<<<1, 32, 0, s>>>(h->a, h->box);
+    return 2;
+  }
+  launch_drift(h, s, fix, 0);
+  launches++;
   if (h->prm.thermostat == MDG_NOSE_HOOVER) {
     const int nbk = blocks_for(n, kBlock);
     k_ke_partial<kBlock><<<nbk, kBlock, 0, s>>>(h->a, n);
     k_zeta<1024><<<1, 1024, 0, s>>>(h->a, h->box, nbk, n, h->prm.aimed_temperature, h->prm.heatbath_tau);
     rec(ev_start);
     // the second drift does not read zeta, so it may precede the zeta update
-    const bool drifted = launch_force_mode<kKickNoseHoover>(h, s, th, true);
+    const bool drifted = launch_force_mode<kKickNoseHoover>(h, s, th, 1);
     rec(ev_stop);
     k_zeta<1024><<<1, 1024, 0, s>>>(h->a, h->box, blocks_for(n, kForceBlock), n,
                                      h->prm.aimed_temperature, h->prm.heatbath_tau);
@@ -258,7 +287,7 @@ int launch_step_tail(mdg_handle *h, cudaStream_t s, cudaEvent_t ev_start, cudaEv
     launches += 1;
   } else {
     rec(ev_start);
-    const bool drifted = launch_force_mode<kKick>(h, s, th, true);
+    const bool drifted = launch_force_mode<kKick>(h, s, th, 1);
     rec(ev_stop);
     launches += 1;
     if (!drifted) {
@@ -344,12 +373,12 @@ mdg_status build_graph(mdg_handle *h) {
     {
       Capture bc{h->cap_stream, body, {}};
       CUDA_TRY(h, begin_capture(bc));
-      launch_build(h, bc.s);
+      launch_build(h, bc.s, fused_step(h) ? fix_buffer(h, s & 1) : nullptr);
       CUDA_TRY(h, end_capture(bc));
     }
     CUDA_TRY(h, begin_capture(c));
     kernels += 2 + launch_step_tail(h, c.s, h->timing ? h->ev[2 * s] : nullptr,
-                                    h->timing ? h->ev[2 * s + 1] : nullptr, true);
+                                    h->timing ? h->ev[2 * s + 1] : nullptr, true, s & 1);
     CUDA_TRY(h, end_capture(c));
   }
   cudaError_t e = cudaGraphInstantiate(&h->exec, g, 0);
@@ -376,16 +405,18 @@ mdg_status step_eager(mdg_handle *h) {
   CUDA_TRY(h, cudaMemcpyAsync(flags, h->d_flags, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   h->kernel_launches++;
+  const int parity = h->fix_buf > 0 ? 1 : 0;
   if (flags[1]) {
-    launch_build(h, h->stream);
-    h->kernel_launches += 9;
+    launch_build(h, h->stream, fused_step(h) ? fix_buffer(h, parity) : nullptr);
+    h->kernel_launches += fused_step(h) ? 10 : 9;
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (h->timing) {
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
   }
-  h->kernel_launches += launch_step_tail(h, h->stream, e0, e1, false);
+  h->kernel_launches += launch_step_tail(h, h->stream, e0, e1, false, parity);
+  if (fused_step(h)) h->fix_buf = 1 - parity;
   CUDA_TRY(h, cudaGetLastError());
   if (h->timing) {
     cudaEventSynchronize(e1);
@@ -412,6 +443,7 @@ mdg_status ensure_list(mdg_handle *h) {
   if (r) return r;
   if (st.error) return translate_device_error(h, st);
   if (!st.list_stale) return MDG_OK;
+  h->fix_buf = -1;  // the rebuild renumbers the atoms
   for (int attempt = 0; attempt < 4; attempt++) {
     launch_build(h, h->stream);
     h->kernel_launches += 9;
@@ -525,6 +557,7 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   if (e == cudaSuccess) e = dalloc(&a.v, cap);
   if (e == cudaSuccess) e = dalloc(&a.q_old, cap);
   if (e == cudaSuccess) e = dalloc(&a.qfix, cap);
+  if (e == cudaSuccess) e = dalloc(&a.qfix2, cap);
   if (e == cudaSuccess) e = dalloc(&a.qloc, cap);
   if (e == cudaSuccess) e = dalloc(&a.ids, cap);
   if (e == cudaSuccess) e = dalloc(&a.type, cap);
@@ -582,6 +615,7 @@ mdg_status mdg_destroy(mdg_handle *h) {
 mdg_status mdg_set_state(mdg_handle *h, const double *q4, const double *v4, const int *type, int n) {
   if (!h || n < 0 || (n > 0 && (!q4 || !v4))) return MDG_ERR_INVALID_ARGUMENT;
   if (n > h->cap) return fail(h, MDG_ERR_CAPACITY, "more atoms than the handle's capacity");
+  h->fix_buf = -1;
   CUDA_TRY(h, cudaSetDevice(h->prm.device));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   if (n > 0) {
@@ -691,6 +725,7 @@ mdg_status mdg_check_expired(mdg_handle *h, int *expired) {
 mdg_status mdg_update_position_half(mdg_handle *h) {
   mdg_status r = check_ready(h);
   if (r) return r;
+  h->fix_buf = -1;  // q, v or the fixed-point copy change outside the fused step
   h->obs_lag = 0.0;
   if (h->n == 0) return MDG_OK;
   launch_drift(h, h->stream, h->prm.precision == MDG_FP32_MIXED, 0);
@@ -701,6 +736,7 @@ mdg_status mdg_update_position_half(mdg_handle *h) {
 mdg_status mdg_calculate_force(mdg_handle *h) {
   mdg_status r = check_ready(h);
   if (r) return r;
+  h->fix_buf = -1;  // q, v or the fixed-point copy change outside the fused step
   h->obs_lag = 0.0;
   if (h->n == 0) return MDG_OK;
   if ((r = ensure_list(h))) return r;
@@ -727,6 +763,7 @@ mdg_status mdg_heatbath_zeta(mdg_handle *h, double t) {
 mdg_status mdg_heatbath_momenta(mdg_handle *h) {
   mdg_status r = check_ready(h);
   if (r) return r;
+  h->fix_buf = -1;  // q, v or the fixed-point copy change outside the fused step
   h->obs_lag = 0.0;
   if (h->n == 0) return MDG_OK;
   k_scale_v<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->n, h->prm.time_step * 0.5);
@@ -737,6 +774,7 @@ mdg_status mdg_heatbath_momenta(mdg_handle *h) {
 mdg_status mdg_langevin(mdg_handle *h) {
   mdg_status r = check_ready(h);
   if (r) return r;
+  h->fix_buf = -1;  // q, v or the fixed-point copy change outside the fused step
   h->obs_lag = 0.0;
   if (h->n == 0) return MDG_OK;
   k_langevin<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n, thermo_of(h));
@@ -754,6 +792,7 @@ mdg_status mdg_set_control(mdg_handle *h, int thermostat, double aimed_temperatu
     h->prm.aimed_temperature = aimed_temperature;
     h->prm.heatbath_tau = heatbath_tau;
     h->prm.heatbath_gamma = heatbath_gamma;
+    h->fix_buf = -1;
     destroy_graph(h);
   }
   return MDG_OK;
@@ -815,6 +854,12 @@ mdg_status mdg_calculate(mdg_handle *h, int nsteps) {
   for (int attempt = 0; attempt < 8; attempt++) {
     long long left = target - st.steps;
     if (left <= 0) break;
+    if (fused_step(h) && h->fix_buf != 0) {
+      // the graph's first step reads buffer 0
+      k_pack_half<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n, h->a.qfix);
+      h->kernel_launches++;
+      h->fix_buf = 0;
+    }
     if (h->use_graphs && left >= kStepsPerGraph && h->graph_dirty) {
       if ((r = build_graph(h))) return r;
     }
@@ -857,6 +902,7 @@ mdg_status mdg_calculate(mdg_handle *h, int nsteps) {
 mdg_status mdg_forces(mdg_handle *h, double *f4) {
   mdg_status r = check_ready(h);
   if (r) return r;
+  h->fix_buf = -1;  // q, v or the fixed-point copy change outside the fused step
   if (h->n == 0) return MDG_OK;
   if (!f4) return MDG_ERR_INVALID_ARGUMENT;
   if ((r = ensure_list(h))) return r;

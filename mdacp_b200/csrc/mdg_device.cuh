@@ -73,6 +73,7 @@ struct Status {
 struct Arrays {
   double4 *q, *v, *q_old;
   int4 *qfix;
+  int4 *qfix2;        // second fixed-point buffer: the fused NVE step reads one and writes the other
   float4 *qloc;       // cell-local FP32 coordinates at the last build (list prefilter)
   int *ids, *type;
   int *cell;          // cell of each slot at the last build
@@ -653,6 +654,19 @@ __global__ void __launch_bounds__(BLOCK) k_drift(Arrays a, Box b, int n, int tra
   if (track_vmax) block_max_to<BLOCK>(&a.st->vmax2_bits, v2);
 }
 
+// Packs q + v dt/2 (the coming step's first half drift) into out without
+// moving atoms: the fixed-point copy the fused NVE force pass reads.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_pack_half(Arrays a, Box b, int n, int4 *out) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= n || a.st->error) return;
+  const double4 q = a.q[i];
+  const double4 v = a.v[i];
+  const double dt2 = b.dt * 0.5;
+  out[i] = make_int4(fixed_coord(dadd(q.x, dmul(v.x, dt2)), b.L[0]), fixed_coord(dadd(q.y, dmul(v.y, dt2)), b.L[1]),
+                     fixed_coord(dadd(q.z, dmul(v.z, dt2)), b.L[2]), 0);
+}
+
 // Writes the fixed-point copy of q without moving atoms.
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_pack_fix(Arrays a, Box b, int n) {
@@ -808,13 +822,20 @@ __device__ __forceinline__ void lj_pair_fp32(const int4 &pi, const int4 &pj, flo
 // folded into an FP64 per-atom sum; the kick is FP64.  With DRIFT the second
 // half drift q += v dt/2 and the |v| maximum of the step are done in the
 // same pass: this kernel reads only the fixed-point copy, so moving q here
-// races with no other thread.
-template <int BLOCK, int MODE, bool DRIFT>
-__global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Thermo th) {
+// races with no other thread.  DRIFT == 2 is the whole NVE step in one pass:
+// qf holds every atom's position after this step's first half drift (packed
+// by the previous step's pass, or by k_pack_half after a rebuild); the
+// kernel applies that drift to its own atom, kicks, drifts again and packs
+// the next step's first-drift position into qf_next (the other buffer, so
+// no thread overwrites a copy that another still reads).  The arithmetic is
+// the separate drift kernels', operation for operation.
+template <int BLOCK, int MODE, int DRIFT>
+__global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Thermo th, const int4 *qf,
+                                                      int4 *qf_next) {
   const int i = blockIdx.x * BLOCK + threadIdx.x;
   double v2 = 0.0, ke = 0.0;
   if (i < n && !a.st->error) {
-    const int4 pi = a.qfix[i];
+    const int4 pi = qf[i];
     const int nn4 = (a.nnbr[i] + 3) & ~3;
     const float sx = b.fix_scale[0], sy = b.fix_scale[1], sz = b.fix_scale[2];
     const unsigned rc2_bits = __float_as_uint(b.rc2f);
@@ -838,10 +859,10 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Th
       m3 = __ldg(row + 7 * st);
     }
     for (int k = 0; k < nn4; k += 4) {
-      const int4 p0 = __ldg(a.qfix + n0);
-      const int4 p1 = __ldg(a.qfix + n1);
-      const int4 p2 = __ldg(a.qfix + n2);
-      const int4 p3 = __ldg(a.qfix + n3);
+      const int4 p0 = __ldg(qf + n0);
+      const int4 p1 = __ldg(qf + n1);
+      const int4 p2 = __ldg(qf + n2);
+      const int4 p3 = __ldg(qf + n3);
       n0 = m0;
       n1 = m1;
       n2 = m2;
@@ -868,17 +889,30 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Th
     Fy += (double)fy;
     Fz += (double)fz;
     const double dt = (MODE == kForceOut) ? 1.0 : b.dt;
+    const double dt2 = b.dt * 0.5;
+    double4 q = a.q[i];
+    if (DRIFT == 2) {
+      // this step's first half drift (the neighbours' copies in qf already have it)
+      const double4 v0 = a.v[i];
+      q.x = dadd(q.x, dmul(v0.x, dt2));
+      q.y = dadd(q.y, dmul(v0.y, dt2));
+      q.z = dadd(q.z, dmul(v0.z, dt2));
+    }
     finish_atom<MODE>(a, b, th, i, Fx * dt, Fy * dt, Fz * dt, v2, ke);
     if (DRIFT) {
       const double4 v = a.v[i];
-      double4 q = a.q[i];
-      const double dt2 = b.dt * 0.5;
       q.x = dadd(q.x, dmul(v.x, dt2));
       q.y = dadd(q.y, dmul(v.y, dt2));
       q.z = dadd(q.z, dmul(v.z, dt2));
       a.q[i] = q;
       v2 = dadd(dadd(dmul(v.x, v.x), dmul(v.y, v.y)), dmul(v.z, v.z));
       if (!isfinite(v2) || !isfinite(q.x + q.y + q.z)) atomicOr(&a.st->error, kErrNonFinite);
+      if (DRIFT == 2) {
+        // the next step's first half drift, packed for its force pass
+        qf_next[i] = make_int4(fixed_coord(dadd(q.x, dmul(v.x, dt2)), b.L[0]),
+                               fixed_coord(dadd(q.y, dmul(v.y, dt2)), b.L[1]),
+                               fixed_coord(dadd(q.z, dmul(v.z, dt2)), b.L[2]), 0);
+      }
     }
   }
   if (MODE == kKickLangevin || DRIFT) warp_max_to(&a.st->vmax2_bits, v2);

@@ -128,10 +128,11 @@ def test_matches_oracle_32k(rho, temperature):
     assert force_error(f32, fo) <= FP32_TOL
 
 
-def test_graph_steps_equal_eager_steps():
+@pytest.mark.parametrize("precision", [M.FP64, M.FP32_MIXED])
+def test_graph_steps_equal_eager_steps(precision):
     g = W.fcc_liquid(6, 0.5, 1.0, seed=21, jitter=0.08, rc=2.5, dt=0.005)
-    a = make_system(g.q, g.v, g.L, g.rc, g.dt)
-    b = make_system(g.q, g.v, g.L, g.rc, g.dt)
+    a = make_system(g.q, g.v, g.L, g.rc, g.dt, precision)
+    b = make_system(g.q, g.v, g.L, g.rc, g.dt, precision)
     a.calculate(40)             # two 20-step graph launches
     for _ in range(40):
         b.calculate(1)          # host-driven steps
@@ -139,6 +140,27 @@ def test_graph_steps_equal_eager_steps():
     qb, vb = b.state_by_id()
     assert np.array_equal(qa, qb) and np.array_equal(va, vb)
     assert a.info()["rebuilds"] == b.info()["rebuilds"]
+
+
+def test_fused_fp32_step_survives_interleaved_calls():
+    # The FP32-mixed NVE step keeps the next step's fixed-point copy between
+    # calls; odd step counts, observers, force queries and a state round
+    # trip in between must leave the trajectory unchanged.
+    g = W.fcc_liquid(6, 0.8442, 1.0, seed=23, jitter=0.05, rc=2.5, dt=0.005)
+    a = make_system(g.q, g.v, g.L, g.rc, g.dt, M.FP32_MIXED)
+    b = make_system(g.q, g.v, g.L, g.rc, g.dt, M.FP32_MIXED)
+    a.calculate(60)
+    b.calculate(7)
+    b.observe()
+    b.calculate(33)
+    b.forces()
+    q, v = b.state_by_id()
+    b.calculate(3)
+    b.pairs()
+    b.calculate(17)
+    qa, va = a.state_by_id()
+    qb, vb = b.state_by_id()
+    assert np.array_equal(qa, qb) and np.array_equal(va, vb)
 
 
 def test_langevin_matches_oracle_noise():
