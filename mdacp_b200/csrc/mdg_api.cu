@@ -19,6 +19,7 @@ namespace {
 
 constexpr int kBlock = 256;       // streaming kernels
 constexpr int kForceBlock = 128;  // pair kernels
+constexpr int kScanBlock = 1024;  // cells per tile of the cell-count scan
 constexpr int kStepsPerGraph = 20;
 
 int blocks_for(int n, int b) { return n > 0 ? (n + b - 1) / b : 1; }
@@ -37,6 +38,7 @@ struct mdg_handle {
   cudaStream_t cap_stream = nullptr;  // capture stream (always owned)
   int *d_flags = nullptr;             // eager-mode conditional values
   double *d_sums = nullptr;           // reduction outputs
+  int *d_tiles = nullptr;             // tile totals of the cell-count scan
   size_t partial_cap = 0;
   bool state_set = false;
   // graph of kStepsPerGraph steps
@@ -181,17 +183,19 @@ void launch_build(mdg_handle *h, cudaStream_t s, int4 *pack = nullptr) {
   k_build_begin<<<1, 32, 0, s>>>(a);
   cudaMemsetAsync(a.cell_count, 0, sizeof(int) * h->ncell, s);
   k_cell_assign<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, h->box, n);
-  k_scan_cells<1024><<<1, 1024, 0, s>>>(a, h->ncell);
+  const int ntiles = blocks_for(h->ncell, kScanBlock);
+  k_scan_tiles<kScanBlock><<<ntiles, kScanBlock, 0, s>>>(a, h->ncell, h->d_tiles);
+  k_scan_tile_sums<kScanBlock><<<1, kScanBlock, 0, s>>>(a, h->ncell, h->d_tiles, ntiles);
+  k_scan_add<kScanBlock><<<ntiles, kScanBlock, 0, s>>>(a, h->ncell, h->d_tiles);
   k_scatter<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, n);
   k_sort_cells<<<blocks_for(h->ncell * 32, kBlock), kBlock, 0, s>>>(a, h->ncell);
-  k_permute<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, h->box, n);
+  k_permute<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, h->box, n, pack);
   cudaMemcpyAsync(a.q, a.q_tmp, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
   cudaMemcpyAsync(a.v, a.v_tmp, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
   cudaMemcpyAsync(a.ids, a.ids_tmp, sizeof(int) * n, cudaMemcpyDeviceToDevice, s);
   cudaMemcpyAsync(a.type, a.type_tmp, sizeof(int) * n, cudaMemcpyDeviceToDevice, s);
   k_build<kForceBlock><<<blocks_for(n, kForceBlock), kForceBlock, 0, s>>>(a, h->box, n);
   k_build_done<<<1, 32, 0, s>>>(a, h->box);
-  if (pack) k_pack_half<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, h->box, n, pack);
 }
 
 // The FP32-mixed NVE step runs as one force pass per step (both half
@@ -257,11 +261,11 @@ int launch_step_tail(mdg_handle *h, cudaStream_t s, cudaEvent_t ev_start, cudaEv
     else cudaEventRecord(e, s);
   };
   if (fused_step(h)) {
+    // one pass: drift, kick, drift, pack and the step counter
     rec(ev_start);
     launch_force_mode<kKick>(h, s, th, 2, fix_buffer(h, parity), fix_buffer(h, 1 - parity));
     rec(ev_stop);
-    k_step_done<<<1, 32, 0, s>>>(h->a, h->box);
-    return 2;
+    return 1;
   }
   launch_drift(h, s, fix, 0);
   launches++;
@@ -356,7 +360,7 @@ mdg_status build_graph(mdg_handle *h) {
     CUDA_TRY(h, cudaGraphConditionalHandleCreate(&hd, g, 0, cudaGraphCondAssignDefault));
     CUDA_TRY(h, cudaGraphConditionalHandleCreate(&hb, g, 0, cudaGraphCondAssignDefault));
     CUDA_TRY(h, begin_capture(c));
-    k_expiry<<<1, 32, 0, c.s>>>(h->a, h->box, hd, 1, h->d_flags);
+    k_expiry<<<1, 32, 0, c.s>>>(h->a, h->box, hd, hb, 1, h->d_flags);
     CUDA_TRY(h, end_capture(c));
     cudaGraph_t body;
     CUDA_TRY(h, add_if(c, hd, &body));
@@ -364,11 +368,9 @@ mdg_status build_graph(mdg_handle *h) {
       Capture bc{h->cap_stream, body, {}};
       CUDA_TRY(h, begin_capture(bc));
       launch_disp(h, bc.s, step_lag(h));
+      k_decide<<<1, 32, 0, bc.s>>>(h->a, hb, 1, h->d_flags);
       CUDA_TRY(h, end_capture(bc));
     }
-    CUDA_TRY(h, begin_capture(c));
-    k_decide<<<1, 32, 0, c.s>>>(h->a, hb, 1, h->d_flags);
-    CUDA_TRY(h, end_capture(c));
     CUDA_TRY(h, add_if(c, hb, &body));
     {
       Capture bc{h->cap_stream, body, {}};
@@ -377,7 +379,7 @@ mdg_status build_graph(mdg_handle *h) {
       CUDA_TRY(h, end_capture(bc));
     }
     CUDA_TRY(h, begin_capture(c));
-    kernels += 2 + launch_step_tail(h, c.s, h->timing ? h->ev[2 * s] : nullptr,
+    kernels += 1 + launch_step_tail(h, c.s, h->timing ? h->ev[2 * s] : nullptr,
                                     h->timing ? h->ev[2 * s + 1] : nullptr, true, s & 1);
     CUDA_TRY(h, end_capture(c));
   }
@@ -393,22 +395,21 @@ mdg_status build_graph(mdg_handle *h) {
 // fine-grained entry points).
 mdg_status step_eager(mdg_handle *h) {
   int flags[2] = {0, 0};
-  k_expiry<<<1, 32, 0, h->stream>>>(h->a, h->box, 0, 0, h->d_flags);
+  k_expiry<<<1, 32, 0, h->stream>>>(h->a, h->box, 0, 0, 0, h->d_flags);
   CUDA_TRY(h, cudaMemcpyAsync(flags, h->d_flags, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   h->kernel_launches++;
   if (flags[0]) {
     launch_disp(h, h->stream, step_lag(h));
-    h->kernel_launches += 3;
+    k_decide<<<1, 32, 0, h->stream>>>(h->a, 0, 0, h->d_flags);
+    CUDA_TRY(h, cudaMemcpyAsync(flags, h->d_flags, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->kernel_launches += 4;
   }
-  k_decide<<<1, 32, 0, h->stream>>>(h->a, 0, 0, h->d_flags);
-  CUDA_TRY(h, cudaMemcpyAsync(flags, h->d_flags, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  h->kernel_launches++;
   const int parity = h->fix_buf > 0 ? 1 : 0;
   if (flags[1]) {
     launch_build(h, h->stream, fused_step(h) ? fix_buffer(h, parity) : nullptr);
-    h->kernel_launches += fused_step(h) ? 10 : 9;
+    h->kernel_launches += 11;
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (h->timing) {
@@ -446,7 +447,7 @@ mdg_status ensure_list(mdg_handle *h) {
   h->fix_buf = -1;  // the rebuild renumbers the atoms
   for (int attempt = 0; attempt < 4; attempt++) {
     launch_build(h, h->stream);
-    h->kernel_launches += 9;
+    h->kernel_launches += 11;
     CUDA_TRY(h, cudaGetLastError());
     r = read_status(h, &st);
     if (r) return r;
@@ -579,6 +580,7 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   if (e == cudaSuccess) e = dalloc(&a.st, 1);
   if (e == cudaSuccess) e = dalloc(&h->d_flags, 4);
   if (e == cudaSuccess) e = dalloc(&h->d_sums, 8);
+  if (e == cudaSuccess) e = dalloc(&h->d_tiles, (size_t)blocks_for(h->ncell, kScanBlock) + 1);
   if (e == cudaSuccess) e = cudaMemsetAsync(a.st, 0, sizeof(Status), h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
@@ -606,6 +608,7 @@ mdg_status mdg_destroy(mdg_handle *h) {
   free_arrays(h->a);
   if (h->d_flags) cudaFree(h->d_flags);
   if (h->d_sums) cudaFree(h->d_sums);
+  if (h->d_tiles) cudaFree(h->d_tiles);
   if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -707,7 +710,7 @@ mdg_status mdg_check_expired(mdg_handle *h, int *expired) {
   if (h->n == 0) return MDG_OK;
   k_vmax<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->n);
   int flags[2] = {0, 0};
-  k_expiry<<<1, 32, 0, h->stream>>>(h->a, h->box, 0, 0, h->d_flags);
+  k_expiry<<<1, 32, 0, h->stream>>>(h->a, h->box, 0, 0, 0, h->d_flags);
   CUDA_TRY(h, cudaMemcpyAsync(flags, h->d_flags, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   if (flags[0]) launch_disp(h, h->stream, h->obs_lag);

@@ -205,9 +205,9 @@ __global__ void __launch_bounds__(BLOCK) k_vmax(Arrays a, int n) {
 // PairList::IsPairListExpired (src/pairlist.cc:25-65): budget -= 2 vmax dt
 // while the budget is positive (a too-fast atom is an error), then arm the
 // displacement check once the budget is spent.  Sets the two conditional
-// handles of this step's graph (or a device flag in eager mode).
-static __global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_disp, int in_graph,
-                         int *eager_flags) {
+// handles of this step's graph (or device flags in eager mode).
+static __global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_disp,
+                                cudaGraphConditionalHandle h_build, int in_graph, int *eager_flags) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   Status *st = a.st;
   int disp = 0, build = 0;
@@ -235,8 +235,16 @@ static __global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_di
   }
   st->want_build = build;
   st->vmax2_bits = 0ull;
-  if (in_graph) cudaGraphSetConditional(h_disp, disp);
-  else eager_flags[0] = disp;
+  // the rebuild decision when no displacement check runs; otherwise k_decide,
+  // after the check, sets it again
+  const int build_now = st->error == 0 && build;
+  if (in_graph) {
+    cudaGraphSetConditional(h_disp, disp);
+    cudaGraphSetConditional(h_build, build_now);
+  } else {
+    eager_flags[0] = disp;
+    eager_flags[1] = build_now;
+  }
 }
 
 // Sets the rebuild condition of this step from the expiry and displacement
@@ -418,29 +426,70 @@ __global__ void __launch_bounds__(BLOCK) k_cell_assign(Arrays a, Box b, int n) {
   a.slot[i] = atomicAdd(&a.cell_count[c], 1);
 }
 
-// Rebuild 2/6: exclusive scan of the cell counts, one block.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_scan_cells(Arrays a, int ncell) {
-  __shared__ int sums[BLOCK];
-  const int t = threadIdx.x;
-  const int chunk = (ncell + BLOCK - 1) / BLOCK;
-  const int beg = min(t * chunk, ncell), end = min(beg + chunk, ncell);
-  int s = 0;
-  for (int c = beg; c < end; c++) s += a.cell_count[c];
-  sums[t] = s;
+__device__ __forceinline__ int block_exclusive_scan(int x, int *total) {
+  __shared__ int warp_tot[BLOCK / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) warp_tot[w] = inc;
   __syncthreads();
-  for (int off = 1; off < BLOCK; off <<= 1) {
-    int x = (t >= off) ? sums[t - off] : 0;
-    __syncthreads();
-    sums[t] += x;
+  if (w == 0) {
+    int t = lane < BLOCK / 32 ? warp_tot[lane] : 0;
+    int ti = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, ti, o);
+      if (lane >= o) ti += y;
+    }
+    if (lane < BLOCK / 32) warp_tot[lane] = ti - t;
+    if (lane == BLOCK / 32 - 1) *total = ti;
+  }
+  __syncthreads();
+  const int r = warp_tot[w] + inc - x;
+  __syncthreads();
+  return r;
+}
+
+// Rebuild 2/6: exclusive scan of the cell counts in three passes -- tiles of
+// BLOCK cells scanned in parallel, the tile totals scanned by one block,
+// the tile offsets added back.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scan_tiles(Arrays a, int ncell, int *tile_sum) {
+  __shared__ int total;
+  if (a.st->error) return;
+  const int c = blockIdx.x * BLOCK + threadIdx.x;
+  const int x = c < ncell ? a.cell_count[c] : 0;
+  const int ex = block_exclusive_scan<BLOCK>(x, &total);
+  if (c < ncell) a.cell_start[c] = ex;
+  if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scan_tile_sums(Arrays a, int ncell, int *tile_sum, int ntiles) {
+  __shared__ int total;
+  if (a.st->error) return;
+  int carry = 0;
+  for (int base = 0; base < ntiles; base += BLOCK) {
+    const int k = base + threadIdx.x;
+    const int x = k < ntiles ? tile_sum[k] : 0;
+    const int ex = block_exclusive_scan<BLOCK>(x, &total);
+    if (k < ntiles) tile_sum[k] = carry + ex;
+    carry += total;
     __syncthreads();
   }
-  int run = sums[t] - s;
-  for (int c = beg; c < end; c++) {
-    a.cell_start[c] = run;
-    run += a.cell_count[c];
-  }
-  if (t == BLOCK - 1) a.cell_start[ncell] = sums[t];
+  if (threadIdx.x == 0) a.cell_start[ncell] = carry;
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scan_add(Arrays a, int ncell, const int *tile_sum) {
+  if (a.st->error) return;
+  const int c = blockIdx.x * BLOCK + threadIdx.x;
+  if (c < ncell && blockIdx.x > 0) a.cell_start[c] += tile_sum[blockIdx.x];
 }
 
 // Rebuild 3/6: scatter old slots to their cell ranges.
@@ -499,7 +548,7 @@ __device__ __forceinline__ int border_bits(const double x[3], const Box &b, int 
 // Rebuild 5/6: gather into cell order (temporary arrays), snapshot q_old
 // (PairList::Init), ghost-strip membership and the total copy count.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_permute(Arrays a, Box b, int n) {
+__global__ void __launch_bounds__(BLOCK) k_permute(Arrays a, Box b, int n, int4 *pack) {
   const int s = blockIdx.x * BLOCK + threadIdx.x;
   int m = 0;
   if (s < n && !a.st->error) {
@@ -518,6 +567,14 @@ __global__ void __launch_bounds__(BLOCK) k_permute(Arrays a, Box b, int n) {
     const int cx = c % b.ms[0], cy = (c / b.ms[0]) % b.ms[1], cz = c / (b.ms[0] * b.ms[1]);
     a.qloc[s] = make_float4((float)(q.x - cx * b.cs[0]), (float)(q.y - cy * b.cs[1]),
                             (float)(q.z - cz * b.cs[2]), 0.f);
+    if (pack) {
+      // the coming step's first-drift positions for the fused FP32 NVE pass
+      const double4 v = a.v[o];
+      const double dt2 = b.dt * 0.5;
+      pack[s] = make_int4(fixed_coord(dadd(q.x, dmul(v.x, dt2)), b.L[0]),
+                          fixed_coord(dadd(q.y, dmul(v.y, dt2)), b.L[1]),
+                          fixed_coord(dadd(q.z, dmul(v.z, dt2)), b.L[2]), 0);
+    }
   }
   const int tot = __reduce_add_sync(0xffffffffu, m);
   if ((threadIdx.x & 31) == 0 && tot) atomicAdd((unsigned long long *)&a.st->total_images, (unsigned long long)tot);
@@ -834,6 +891,11 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Th
                                                       int4 *qf_next) {
   const int i = blockIdx.x * BLOCK + threadIdx.x;
   double v2 = 0.0, ke = 0.0;
+  if (DRIFT == 2 && MODE == kKick && i == 0 && !a.st->error) {
+    // the step counter (k_step_done's work): nothing in this pass reads it
+    a.st->steps++;
+    a.st->sim_time += b.dt;
+  }
   if (i < n && !a.st->error) {
     const int4 pi = qf[i];
     const int nn4 = (a.nnbr[i] + 3) & ~3;
