@@ -243,6 +243,33 @@ mdg_status mdg_ensemble_rebuilds(mdg_ensemble *e, int64_t *rebuilds, int64_t *st
 mdg_status mdg_ensemble_set_graph_mode(mdg_ensemble *e, int use_graphs);
 void *mdg_ensemble_stream(mdg_ensemble *e);
 
+/* ---------------------------------------------------------- adjoint
+ * Gradients of a trajectory loss, by a reverse sweep over the steps
+ * (mdacp_b200/csrc/mdg_adjoint.cu).  No counterpart in the reference, which
+ * computes no gradients.  Potential U(r) = epsilon phi(r/sigma) with the
+ * reference's smoothed phi (src/variables.cc:16-33) and the cut-off in units
+ * of sigma; steps as MDManager::Calculate (NVE, src/mdmanager.cc:153-186), in
+ * FP64.  Loss L = 1/(steps n) sum over the steps' end states of
+ * [PE + sum over pairs g((r-lo)/w) g((hi-r)/w)], g the logistic function. */
+typedef struct mdg_adjoint_params {
+  double L[3];
+  double cutoff;          /* in units of sigma (CUTOFF_LENGTH, include/mdconfig.h:31) */
+  double time_step;
+  double epsilon, sigma;
+  double shell_lo, shell_hi, shell_width;  /* smoothed pair count window */
+  int steps;
+  int checkpoint_every;   /* states kept every k steps; segments recomputed */
+  int device;
+} mdg_adjoint_params;
+
+void mdg_adjoint_default_params(mdg_adjoint_params *p);
+/* q0, v0: n x 3 doubles.  loss is required; with all three gradient
+ * pointers NULL only the forward pass runs.  dloss_dq0: n x 3 doubles.
+ * Allocates its device memory per call (checkpoints: 2 x 32 B per atom per
+ * checkpoint). */
+mdg_status mdg_adjoint_run(const mdg_adjoint_params *p, const double *q0, const double *v0, int n, double *loss,
+                           double *dloss_deps, double *dloss_dsigma, double *dloss_dq0);
+
 const char *mdg_last_error(mdg_handle *h);
 const char *mdg_status_string(mdg_status s);
 /* Library version string. */

@@ -19,6 +19,7 @@ __all__ = [
     "Params",
     "Info",
     "Replica",
+    "AdjointParams",
     "System",
     "Ensemble",
     "load_library",
@@ -101,6 +102,24 @@ class Info(ctypes.Structure):
                 for name, _ in self._fields_}
 
 
+class AdjointParams(ctypes.Structure):
+    """Mirror of mdg_adjoint_params (include/mdacp_b200.h)."""
+
+    _fields_ = [
+        ("L", ctypes.c_double * 3),
+        ("cutoff", ctypes.c_double),
+        ("time_step", ctypes.c_double),
+        ("epsilon", ctypes.c_double),
+        ("sigma", ctypes.c_double),
+        ("shell_lo", ctypes.c_double),
+        ("shell_hi", ctypes.c_double),
+        ("shell_width", ctypes.c_double),
+        ("steps", ctypes.c_int),
+        ("checkpoint_every", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
 class Replica(ctypes.Structure):
     """``mdg_replica`` (include/mdacp_b200.h)."""
 
@@ -113,6 +132,8 @@ _DP = ctypes.POINTER(ctypes.c_double)
 _IP = ctypes.POINTER(ctypes.c_int)
 _I64P = ctypes.POINTER(ctypes.c_int64)
 SIGNATURES = {
+    "mdg_adjoint_default_params": (None, [ctypes.POINTER(AdjointParams)]),
+    "mdg_adjoint_run": (ctypes.c_int, [ctypes.POINTER(AdjointParams), _DP, _DP, ctypes.c_int, _DP, _DP, _DP, _DP]),
     "mdg_default_params": (None, [ctypes.POINTER(Params)]),
     "mdg_create": (ctypes.c_int, [ctypes.POINTER(Params), ctypes.POINTER(_H)]),
     "mdg_destroy": (ctypes.c_int, [_H]),
