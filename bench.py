@@ -203,13 +203,20 @@ def main():
                     help="NVE steps of the energy-drift comparison of the two paths (0: skip)")
     ap.add_argument("--eager", action="store_true",
                     help="launch every kernel from the host instead of CUDA graphs (for profilers)")
-    ap.add_argument("--config", choices=["c2", "c1", "c3", "c4"], default="c2",
+    ap.add_argument("--config", choices=["c2", "c1", "c3", "c4", "c5"], default="c2",
                     help="c2: 2.05M-atom liquid (headline); c1: 32k atoms rho 0.5; c3: 1M-atom Langevin slab; "
-                         "c4: 256-replica ensemble")
+                         "c4: 256-replica ensemble; c5: adjoint gradients of a 32k-atom trajectory")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.config == "c4":
         return main_ensemble(args, ws, rank, local)
+    if args.config == "c5":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference computes no gradients "
+                                  "(no adjoint or differentiable path)"}), flush=True)
+            return 0
+        return main_adjoint(args, ws, rank, local)
     state, config = workload(args, rank)
     if args.impl == "reference":
         return main_reference(args, ws, rank, state, config)
@@ -479,6 +486,73 @@ def main_mdg(args, ws, rank, local, state, config):
         except Exception as exc:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                                     "sample": f"not run: {exc}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main_adjoint(args, ws, rank, local):
+    """Gradients of a 200-step trajectory loss (32,000 atoms, rho 0.8442,
+    T 1.0, FP64, checkpoints every 20 steps) with respect to epsilon, sigma
+    and the initial positions; checked against central finite differences."""
+    import torch
+
+    from mdacp_b200 import adjoint as A
+    from mdacp_b200 import workloads as W
+
+    dist = init_dist(ws, "nccl")
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    st = W.config_c5(seed=55 + rank)
+    n, T, k = st.n, 200, 20
+    kw = dict(steps=T, checkpoint_every=k, time_step=st.dt, device=local)
+    per_tpa = {}
+    for t in (1, 2, 4, 8):  # the lane counts the autotuner chooses from
+        A.trajectory_gradients(st.q, st.v, st.L, threads_per_atom=t, **kw)
+        t0 = time.perf_counter()
+        A.trajectory_gradients(st.q, st.v, st.L, threads_per_atom=t, **kw)
+        per_tpa[t] = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        A.trajectory_gradients(st.q, st.v, st.L, **kw)
+    barrier(dist, device)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        loss, de, ds, dq = A.trajectory_gradients(st.q, st.v, st.L, **kw)
+    t_grad = max_over_ranks(dist, (time.perf_counter() - t0) / args.steps, device)
+    t0 = time.perf_counter()
+    A.trajectory_loss(st.q, st.v, st.L, **kw)
+    t_fwd = time.perf_counter() - t0
+    h = 1e-6
+    f = lambda qq, e=1.0, s=1.0: A.trajectory_loss(qq, st.v, st.L, epsilon=e, sigma=s, **kw)  # noqa: E731
+    d = np.random.default_rng(11).standard_normal(st.q.shape)
+    d /= np.linalg.norm(d)
+    g = dq / np.linalg.norm(dq)
+    fd = {"epsilon": (f(st.q, 1 + h) - f(st.q, 1 - h)) / (2 * h),
+          "sigma": (f(st.q, 1.0, 1 + h) - f(st.q, 1.0, 1 - h)) / (2 * h),
+          "q0_along_gradient": (f(st.q + h * g) - f(st.q - h * g)) / (2 * h),
+          "q0_random_direction": (f(st.q + h * d) - f(st.q - h * d)) / (2 * h)}
+    adj = {"epsilon": de, "sigma": ds, "q0_along_gradient": float(np.linalg.norm(dq)),
+           "q0_random_direction": float((dq * d).sum())}
+    rel = {key: abs(adj[key] - fd[key]) / abs(fd[key]) for key in fd}
+    value = ws * n * T / t_grad
+    line = {
+        "metric": "adjoint atom-steps/s (forward + reverse sweep), 32,000-atom LJ, 200 FP64 steps",
+        "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_grad * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "lj_fcc32000_rho0.8442: 32000 atoms, FCC 20^3 cells, T 1.0, rc 2.5 sigma, dt 0.005, "
+                               "200 NVE steps, checkpoints every 20 steps, loss = time-averaged PE + smoothed pair "
+                               "count in 1.0 < r < 1.5, per atom", "n_atoms": n, "md_steps": T,
+                   "checkpoint_every": k},
+        "forward_only": {"value": n * T / t_fwd, "unit": UNIT, "seconds": t_fwd},
+        "gradient_check": {"h": h, "adjoint": adj, "finite_difference": fd, "relative_error": rel},
+        "seconds_per_lanes_per_atom": {str(t): v for t, v in per_tpa.items()},
+        "timing": "host wall clock around the C-ABI call (host-driven steps, device sums read once per run)",
+        "cpu_baseline": {"value": None, "unit": UNIT, "cores": None, "kind": "port",
+                         "sample": "not run: the reference computes no gradients"},
+    }
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -259,6 +259,8 @@ typedef struct mdg_adjoint_params {
   double shell_lo, shell_hi, shell_width;  /* smoothed pair count window */
   int steps;
   int checkpoint_every;   /* states kept every k steps; segments recomputed */
+  int threads_per_atom;   /* lanes per atom in the pair kernels: 1, 2, 4, 8, or 0 to
+                             time all four once per device and problem shape */
   int device;
 } mdg_adjoint_params;
 

@@ -116,6 +116,7 @@ class AdjointParams(ctypes.Structure):
         ("shell_width", ctypes.c_double),
         ("steps", ctypes.c_int),
         ("checkpoint_every", ctypes.c_int),
+        ("threads_per_atom", ctypes.c_int),
         ("device", ctypes.c_int),
     ]
 

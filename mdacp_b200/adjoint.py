@@ -31,7 +31,7 @@ _DP = ctypes.POINTER(ctypes.c_double)
 
 
 def params(L, steps=200, checkpoint_every=20, time_step=0.005, epsilon=1.0, sigma=1.0, cutoff=2.5,
-           shell=(1.0, 1.5, 0.05), device=0) -> AdjointParams:
+           shell=(1.0, 1.5, 0.05), threads_per_atom=0, device=0) -> AdjointParams:
     lib = load_library()
     p = AdjointParams()
     lib.mdg_adjoint_default_params(ctypes.byref(p))
@@ -43,6 +43,7 @@ def params(L, steps=200, checkpoint_every=20, time_step=0.005, epsilon=1.0, sigm
     p.sigma = float(sigma)
     p.cutoff = float(cutoff)
     p.shell_lo, p.shell_hi, p.shell_width = (float(x) for x in shell)
+    p.threads_per_atom = int(threads_per_atom)
     p.device = int(device)
     return p
 

@@ -33,7 +33,10 @@
 
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "mdacp_b200.h"
@@ -97,32 +100,39 @@ __device__ __forceinline__ int cell_of(const double4 &q, const Grid &g) {
 }
 
 // Calls f(j, d, r) for every partner j != i with r < r_c, d = minimum image of
-// q_i - q_j; the 27 cells around i's, each in index order.
-template <class F>
-__device__ __forceinline__ void for_pairs(const double4 *q, const Grid &g, const Pot &p, int i, F f) {
+// q_i - q_j, over the 27 cells around i's, each in index order.  TPA lanes
+// share one atom: lane `sub` takes cells sub, sub + TPA, ... of the 27 (the
+// caller combines the lanes' sums with group_sum).
+template <int TPA, class F>
+__device__ __forceinline__ void for_pairs(const double4 *q, const Grid &g, const Pot &p, int i, int sub, F f) {
   const double4 qi = q[i];
   const int cx = cell_axis(qi.x, g.L[0], g.inv_cs[0], g.ms[0]);
   const int cy = cell_axis(qi.y, g.L[1], g.inv_cs[1], g.ms[1]);
   const int cz = cell_axis(qi.z, g.L[2], g.inv_cs[2], g.ms[2]);
-  for (int dz = -1; dz <= 1; dz++) {
-    const int z = (cz + dz + g.ms[2]) % g.ms[2];
-    for (int dy = -1; dy <= 1; dy++) {
-      const int y = (cy + dy + g.ms[1]) % g.ms[1];
-      for (int dx = -1; dx <= 1; dx++) {
-        const int x = (cx + dx + g.ms[0]) % g.ms[0];
-        const int c = (z * g.ms[1] + y) * g.ms[0] + x;
-        for (int k = g.start[c]; k < g.start[c + 1]; k++) {
-          const int j = g.perm[k];
-          if (j == i) continue;
-          const double4 qj = q[j];
-          double d[3] = {qi.x - qj.x, qi.y - qj.y, qi.z - qj.z};
-          for (int a = 0; a < 3; a++) d[a] -= g.L[a] * rint(d[a] / g.L[a]);
-          const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-          if (r2 < p.rc2) f(j, d, sqrt(r2));
-        }
-      }
+  for (int nbh = sub; nbh < 27; nbh += TPA) {
+    const int z = (cz + nbh / 9 - 1 + g.ms[2]) % g.ms[2];
+    const int y = (cy + (nbh / 3) % 3 - 1 + g.ms[1]) % g.ms[1];
+    const int x = (cx + nbh % 3 - 1 + g.ms[0]) % g.ms[0];
+    const int c = (z * g.ms[1] + y) * g.ms[0] + x;
+    for (int k = g.start[c]; k < g.start[c + 1]; k++) {
+      const int j = g.perm[k];
+      if (j == i) continue;
+      const double4 qj = q[j];
+      double d[3] = {qi.x - qj.x, qi.y - qj.y, qi.z - qj.z};
+      for (int a = 0; a < 3; a++) d[a] -= g.L[a] * rint(d[a] / g.L[a]);
+      const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      if (r2 < p.rc2) f(j, d, sqrt(r2));
     }
   }
+}
+
+// Sum over the TPA lanes of one atom (fixed butterfly order); every lane of
+// the group gets the total.
+template <int TPA>
+__device__ __forceinline__ double group_sum(double x) {
+#pragma unroll
+  for (int o = 1; o < TPA; o <<= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
 }
 
 // Fixed-order block sum of NS values into part[blockIdx.x * NS + k].
@@ -201,29 +211,38 @@ __global__ void a_sort(int ncell, const int *start, int *perm) {
 }
 
 // --------------------------------------------------------------- physics
-__global__ void a_force(const double4 *q, int n, Grid g, Pot p, double4 *f) {
-  const int i = blockIdx.x * kAB + threadIdx.x;
-  if (i >= n) return;
+template <int TPA>
+__global__ void __launch_bounds__(kAB) a_force(const double4 *q, int n, Grid g, Pot p, double4 *f) {
+  const int t = blockIdx.x * kAB + threadIdx.x;
+  const int i = t / TPA, sub = t % TPA;
   double fx = 0.0, fy = 0.0, fz = 0.0;
-  for_pairs(q, g, p, i, [&](int, const double *d, double r) {
-    double u, u1, u2;
-    pair_u(r, p, u, u1, u2);
-    const double c = -u1 / r;
-    fx += c * d[0];
-    fy += c * d[1];
-    fz += c * d[2];
-  });
-  f[i] = make_double4(fx, fy, fz, 0.0);
+  if (i < n) {
+    for_pairs<TPA>(q, g, p, i, sub, [&](int, const double *d, double r) {
+      double u, u1, u2;
+      pair_u(r, p, u, u1, u2);
+      const double c = -u1 / r;
+      fx += c * d[0];
+      fy += c * d[1];
+      fz += c * d[2];
+    });
+  }
+  fx = group_sum<TPA>(fx);
+  fy = group_sum<TPA>(fy);
+  fz = group_sum<TPA>(fz);
+  if (i < n && sub == 0) f[i] = make_double4(fx, fy, fz, 0.0);
 }
 
 // Loss terms at q: per-block sums of PE, S and dPE/dsigma (pairs counted from
 // both ends, halved); with grad, dL_t/dq_i * scale added into lq.
-__global__ void a_loss(const double4 *q, int n, Grid g, Pot p, double *part, double4 *lq, double scale) {
-  const int i = blockIdx.x * kAB + threadIdx.x;
+template <int TPA>
+__global__ void __launch_bounds__(kAB) a_loss(const double4 *q, int n, Grid g, Pot p, double *part, double4 *lq,
+                                              double scale) {
+  const int t = blockIdx.x * kAB + threadIdx.x;
+  const int i = t / TPA, sub = t % TPA;
   double v[3] = {0.0, 0.0, 0.0};
+  double gx = 0.0, gy = 0.0, gz = 0.0;
   if (i < n) {
-    double gx = 0.0, gy = 0.0, gz = 0.0;
-    for_pairs(q, g, p, i, [&](int, const double *d, double r) {
+    for_pairs<TPA>(q, g, p, i, sub, [&](int, const double *d, double r) {
       double u, u1, u2, s, s1;
       pair_u(r, p, u, u1, u2);
       shell(r, p, s, s1);
@@ -235,7 +254,12 @@ __global__ void a_loss(const double4 *q, int n, Grid g, Pot p, double *part, dou
       gy += c * d[1];
       gz += c * d[2];
     });
-    if (lq) {
+  }
+  if (lq) {
+    gx = group_sum<TPA>(gx);
+    gy = group_sum<TPA>(gy);
+    gz = group_sum<TPA>(gz);
+    if (i < n && sub == 0) {
       double4 l = lq[i];
       l.x += scale * gx;
       l.y += scale * gy;
@@ -248,13 +272,16 @@ __global__ void a_loss(const double4 *q, int n, Grid g, Pot p, double *part, dou
 
 // w = H(q) u (pair energy Hessian times u); per-block sums of
 // sum_i u_i . dF_i/d(eps, sigma).
-__global__ void a_hvp(const double4 *q, int n, Grid g, Pot p, const double4 *u, double4 *w, double *part) {
-  const int i = blockIdx.x * kAB + threadIdx.x;
+template <int TPA>
+__global__ void __launch_bounds__(kAB) a_hvp(const double4 *q, int n, Grid g, Pot p, const double4 *u, double4 *w,
+                                             double *part) {
+  const int t = blockIdx.x * kAB + threadIdx.x;
+  const int i = t / TPA, sub = t % TPA;
   double v[2] = {0.0, 0.0};
+  double wx = 0.0, wy = 0.0, wz = 0.0;
   if (i < n) {
     const double4 ui = u[i];
-    double wx = 0.0, wy = 0.0, wz = 0.0;
-    for_pairs(q, g, p, i, [&](int j, const double *d, double r) {
+    for_pairs<TPA>(q, g, p, i, sub, [&](int j, const double *d, double r) {
       double uu, u1, u2;
       pair_u(r, p, uu, u1, u2);
       const double4 uj = u[j];
@@ -271,9 +298,21 @@ __global__ void a_hvp(const double4 *q, int n, Grid g, Pot p, const double4 *u, 
       v[0] += -(u1 / p.eps) * eu;
       v[1] += (u1 + r * u2) / p.sigma * eu;
     });
-    w[i] = make_double4(wx, wy, wz, 0.0);
   }
+  wx = group_sum<TPA>(wx);
+  wy = group_sum<TPA>(wy);
+  wz = group_sum<TPA>(wz);
+  if (i < n && sub == 0) w[i] = make_double4(wx, wy, wz, 0.0);
   block_sums<2>(v, part);
+}
+
+// Fixed-order sum of nb blocks' NS partials into out[k] (one warp); the
+// per-step sums stay on the device until the end of the run.
+__global__ void a_reduce(const double *part, int nb, int ns, double *out) {
+  if (threadIdx.x >= ns) return;
+  double x = 0.0;
+  for (int b = 0; b < nb; b++) x += part[(size_t)b * ns + threadIdx.x];
+  out[threadIdx.x] = x;
 }
 
 // --------------------------------------------------------- integration
@@ -332,7 +371,7 @@ __global__ void a_rev2(double4 *lq, double4 *lv, const double4 *w, int n, double
 int nblk(int n) { return n > 0 ? (n + kAB - 1) / kAB : 1; }
 
 struct Run {
-  int n = 0, ncell = 0, nb = 0;
+  int n = 0, ncell = 0, tpa = 1;
   cudaStream_t s = nullptr;
   Grid g{};
   Pot p{};
@@ -342,9 +381,10 @@ struct Run {
   double4 *ck_q = nullptr, *ck_v = nullptr;    // checkpoints
   double4 *seg_qh = nullptr, *seg_v = nullptr;  // one segment's q_h and v'
   int *cell = nullptr, *count = nullptr, *start = nullptr, *fill = nullptr, *perm = nullptr;
-  double *part = nullptr;
+  double *part = nullptr;                       // block partials of the pair kernels
+  double *loss_sums = nullptr;                  // per step: PE, S, dPE/dsigma
+  double *adj_sums = nullptr;                   // per reverse step: u . dF/d(eps, sigma)
   std::vector<void *> owned;
-  std::string err;
 
   template <typename T>
   cudaError_t alloc(T **ptr, size_t count_) {
@@ -356,6 +396,7 @@ struct Run {
     for (void *x : owned) cudaFree(x);
     if (s) cudaStreamDestroy(s);
   }
+  int pair_blocks() const { return (int)(((long long)n * tpa + kAB - 1) / kAB); }
 
   // cell grid of the positions x
   void cells(const double4 *x) {
@@ -366,30 +407,91 @@ struct Run {
     a_fill<<<nblk(n), kAB, 0, s>>>(n, cell, start, fill, perm);
     a_sort<<<nblk(ncell), kAB, 0, s>>>(ncell, start, perm);
   }
+  void force(const double4 *x) {
+    const int nb = pair_blocks();
+    switch (tpa) {
+      case 1: a_force<1><<<nb, kAB, 0, s>>>(x, n, g, p, f); break;
+      case 2: a_force<2><<<nb, kAB, 0, s>>>(x, n, g, p, f); break;
+      case 4: a_force<4><<<nb, kAB, 0, s>>>(x, n, g, p, f); break;
+      default: a_force<8><<<nb, kAB, 0, s>>>(x, n, g, p, f); break;
+    }
+  }
+  void loss(const double4 *x, double4 *grad, double scale) {
+    const int nb = pair_blocks();
+    switch (tpa) {
+      case 1: a_loss<1><<<nb, kAB, 0, s>>>(x, n, g, p, part, grad, scale); break;
+      case 2: a_loss<2><<<nb, kAB, 0, s>>>(x, n, g, p, part, grad, scale); break;
+      case 4: a_loss<4><<<nb, kAB, 0, s>>>(x, n, g, p, part, grad, scale); break;
+      default: a_loss<8><<<nb, kAB, 0, s>>>(x, n, g, p, part, grad, scale); break;
+    }
+  }
+  void hvp(const double4 *x) {
+    const int nb = pair_blocks();
+    switch (tpa) {
+      case 1: a_hvp<1><<<nb, kAB, 0, s>>>(x, n, g, p, u, w, part); break;
+      case 2: a_hvp<2><<<nb, kAB, 0, s>>>(x, n, g, p, u, w, part); break;
+      case 4: a_hvp<4><<<nb, kAB, 0, s>>>(x, n, g, p, u, w, part); break;
+      default: a_hvp<8><<<nb, kAB, 0, s>>>(x, n, g, p, u, w, part); break;
+    }
+  }
   // one forward step; keeps q_h and v' when asked
   void step(double4 *qh_out, double4 *v_out) {
     a_drift<<<nblk(n), kAB, 0, s>>>(q, v, n, 0.5 * dt);
     cells(q);
-    a_force<<<nblk(n), kAB, 0, s>>>(q, n, g, p, f);
+    force(q);
     if (qh_out) cudaMemcpyAsync(qh_out, q, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
     a_kick<<<nblk(n), kAB, 0, s>>>(v, f, n, dt);
     if (v_out) cudaMemcpyAsync(v_out, v, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
     a_drift<<<nblk(n), kAB, 0, s>>>(q, v, n, 0.5 * dt);
   }
-  // loss terms at x (sums appended to host), gradient into lq when scale != 0
-  cudaError_t loss_at(const double4 *x, double scale, std::vector<double> &sums) {
+  // loss terms at x: sums into out[0..2] (device), gradient into lq when scale != 0
+  void loss_at(const double4 *x, double scale, double *out) {
     cells(x);
-    a_loss<<<nb, kAB, 0, s>>>(x, n, g, p, part, scale != 0.0 ? lq : nullptr, scale);
-    std::vector<double> h((size_t)nb * 3);
-    cudaError_t e = cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    double t[3] = {0.0, 0.0, 0.0};
-    for (int b = 0; b < nb; b++)
-      for (int k = 0; k < 3; k++) t[k] += h[(size_t)b * 3 + k];
-    sums.insert(sums.end(), t, t + 3);
-    return e;
+    loss(x, scale != 0.0 ? lq : nullptr, scale);
+    if (out) a_reduce<<<1, 32, 0, s>>>(part, pair_blocks(), 3, out);
   }
 };
+
+// Lanes per atom of the pair kernels, chosen once per device and problem
+// shape by timing the force kernel with 1, 2, 4 and 8 lanes (the fastest is
+// kept for the process, so repeated runs of one shape use the same lanes and
+// give the same sums).
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, int>, int> g_tune;
+
+int autotune_tpa(Run &R, int device) {
+  const auto key = std::make_tuple(device, R.n, R.ncell);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second;
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  R.cells(R.q);
+  int best = 1;
+  float best_ms = 1e30f;
+  for (int t : {1, 2, 4, 8}) {
+    R.tpa = t;
+    R.force(R.q);  // warm-up
+    cudaEventRecord(e0, R.s);
+    for (int r = 0; r < 3; r++) R.force(R.q);
+    cudaEventRecord(e1, R.s);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune[key] = best;
+  return best;
+}
 
 }  // namespace
 
@@ -408,6 +510,7 @@ void mdg_adjoint_default_params(mdg_adjoint_params *p) {
   p->shell_width = 0.05;
   p->steps = 200;
   p->checkpoint_every = 20;
+  p->threads_per_atom = 0;
   p->device = 0;
 }
 
@@ -415,7 +518,9 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
                            double *dloss_deps, double *dloss_dsigma, double *dloss_dq0) {
   if (!prm || !q0 || !v0 || !loss || n < 1 || prm->steps < 1 || prm->checkpoint_every < 1 ||
       !(prm->time_step > 0.0) || !(prm->epsilon > 0.0) || !(prm->sigma > 0.0) || !(prm->cutoff > 0.0) ||
-      !(prm->shell_width > 0.0))
+      !(prm->shell_width > 0.0) ||
+      (prm->threads_per_atom != 0 && prm->threads_per_atom != 1 && prm->threads_per_atom != 2 &&
+       prm->threads_per_atom != 4 && prm->threads_per_atom != 8))
     return MDG_ERR_INVALID_ARGUMENT;
   const bool grad = dloss_deps || dloss_dsigma || dloss_dq0;
   int ndev = 0;
@@ -445,9 +550,9 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   R.p.a = prm->shell_lo;
   R.p.b = prm->shell_hi;
   R.p.w = prm->shell_width;
-  R.nb = nblk(n);
   const int T = prm->steps, k = prm->checkpoint_every;
   const int nck = (T + k - 1) / k + 1;
+  const size_t max_blocks = ((size_t)n * 8 + kAB - 1) / kAB;
 
   cudaError_t e = cudaStreamCreateWithFlags(&R.s, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = R.alloc(&R.q, n);
@@ -459,12 +564,14 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   if (e == cudaSuccess) e = R.alloc(&R.fill, R.ncell);
   if (e == cudaSuccess) e = R.alloc(&R.start, R.ncell + 1);
   if (e == cudaSuccess) e = R.alloc(&R.perm, n);
-  if (e == cudaSuccess) e = R.alloc(&R.part, (size_t)R.nb * 3);
+  if (e == cudaSuccess) e = R.alloc(&R.part, max_blocks * 3);
+  if (e == cudaSuccess) e = R.alloc(&R.loss_sums, (size_t)T * 3);
   if (grad) {
     if (e == cudaSuccess) e = R.alloc(&R.lq, n);
     if (e == cudaSuccess) e = R.alloc(&R.lv, n);
     if (e == cudaSuccess) e = R.alloc(&R.u, n);
     if (e == cudaSuccess) e = R.alloc(&R.w, n);
+    if (e == cudaSuccess) e = R.alloc(&R.adj_sums, (size_t)T * 2);
     if (e == cudaSuccess) e = R.alloc(&R.ck_q, (size_t)nck * n);
     if (e == cudaSuccess) e = R.alloc(&R.ck_v, (size_t)nck * n);
     if (e == cudaSuccess) e = R.alloc(&R.seg_qh, (size_t)k * n);
@@ -486,18 +593,21 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
     if (e == cudaSuccess) e = cudaStreamSynchronize(R.s);
     if (e != cudaSuccess) return MDG_ERR_CUDA;
   }
+  R.tpa = prm->threads_per_atom ? prm->threads_per_atom : autotune_tpa(R, prm->device);
 
   // forward pass: loss terms per step, checkpoints every k steps
-  std::vector<double> sums;
-  sums.reserve((size_t)3 * T);
   for (int t = 0; t < T; t++) {
     if (grad && t % k == 0) {
       cudaMemcpyAsync(R.ck_q + (size_t)(t / k) * n, R.q, sizeof(double4) * n, cudaMemcpyDeviceToDevice, R.s);
       cudaMemcpyAsync(R.ck_v + (size_t)(t / k) * n, R.v, sizeof(double4) * n, cudaMemcpyDeviceToDevice, R.s);
     }
     R.step(nullptr, nullptr);
-    if (R.loss_at(R.q, 0.0, sums) != cudaSuccess) return MDG_ERR_CUDA;
+    R.loss_at(R.q, 0.0, R.loss_sums + (size_t)3 * t);
   }
+  std::vector<double> sums((size_t)T * 3);
+  e = cudaMemcpyAsync(sums.data(), R.loss_sums, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, R.s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(R.s);
+  if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return MDG_ERR_CUDA;
   const double norm = 1.0 / ((double)T * n);
   double l = 0.0, dl_deps = 0.0, dl_dsig = 0.0;
   for (int t = 0; t < T; t++) {
@@ -506,15 +616,13 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
     dl_dsig += sums[3 * t + 2];
   }
   *loss = l * norm;
-  if (!grad) return cudaGetLastError() == cudaSuccess ? MDG_OK : MDG_ERR_CUDA;
+  if (!grad) return MDG_OK;
   dl_deps *= norm;
   dl_dsig *= norm;
 
   // reverse sweep, one checkpointed segment at a time
   cudaMemsetAsync(R.lq, 0, sizeof(double4) * n, R.s);
   cudaMemsetAsync(R.lv, 0, sizeof(double4) * n, R.s);
-  std::vector<double> scratch;
-  std::vector<double> hp((size_t)R.nb * 2);
   for (int seg = (T - 1) / k; seg >= 0; seg--) {
     const int t0 = seg * k, t1 = std::min(T, t0 + k);
     cudaMemcpyAsync(R.q, R.ck_q + (size_t)seg * n, sizeof(double4) * n, cudaMemcpyDeviceToDevice, R.s);
@@ -526,26 +634,26 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
       // q' = q_h + v' dt/2, and this step's loss gradient at q'
       cudaMemcpyAsync(R.tmp, qh, sizeof(double4) * n, cudaMemcpyDeviceToDevice, R.s);
       a_drift<<<nblk(n), kAB, 0, R.s>>>(R.tmp, vp, n, 0.5 * R.dt);
-      scratch.clear();
-      if (R.loss_at(R.tmp, norm, scratch) != cudaSuccess) return MDG_ERR_CUDA;
+      R.loss_at(R.tmp, norm, nullptr);
       a_rev1<<<nblk(n), kAB, 0, R.s>>>(R.lq, R.lv, R.u, n, R.dt);
       R.cells(qh);
-      a_hvp<<<R.nb, kAB, 0, R.s>>>(qh, n, R.g, R.p, R.u, R.w, R.part);
-      e = cudaMemcpyAsync(hp.data(), R.part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, R.s);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(R.s);
-      if (e != cudaSuccess) return MDG_ERR_CUDA;
-      for (int b = 0; b < R.nb; b++) {
-        dl_deps += hp[(size_t)b * 2];
-        dl_dsig += hp[(size_t)b * 2 + 1];
-      }
+      R.hvp(qh);
+      a_reduce<<<1, 32, 0, R.s>>>(R.part, R.pair_blocks(), 2, R.adj_sums + (size_t)2 * t);
       a_rev2<<<nblk(n), kAB, 0, R.s>>>(R.lq, R.lv, R.w, n, R.dt);
     }
   }
+  std::vector<double> adj((size_t)T * 2);
+  e = cudaMemcpyAsync(adj.data(), R.adj_sums, sizeof(double) * adj.size(), cudaMemcpyDeviceToHost, R.s);
+  std::vector<double4> h(n);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), R.lq, sizeof(double4) * n, cudaMemcpyDeviceToHost, R.s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(R.s);
+  if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return MDG_ERR_CUDA;
+  // dynamics terms summed in reverse-sweep order, as the sweep produced them
+  for (int t = T - 1; t >= 0; t--) {
+    dl_deps += adj[(size_t)2 * t];
+    dl_dsig += adj[(size_t)2 * t + 1];
+  }
   if (dloss_dq0) {
-    std::vector<double4> h(n);
-    e = cudaMemcpyAsync(h.data(), R.lq, sizeof(double4) * n, cudaMemcpyDeviceToHost, R.s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(R.s);
-    if (e != cudaSuccess) return MDG_ERR_CUDA;
     for (int i = 0; i < n; i++) {
       dloss_dq0[3 * i] = h[i].x;
       dloss_dq0[3 * i + 1] = h[i].y;
@@ -554,7 +662,7 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   }
   if (dloss_deps) *dloss_deps = dl_deps;
   if (dloss_dsigma) *dloss_dsigma = dl_dsig;
-  return cudaGetLastError() == cudaSuccess ? MDG_OK : MDG_ERR_CUDA;
+  return MDG_OK;
 }
 
 }  // extern "C"
