@@ -243,6 +243,39 @@ mdg_status mdg_ensemble_rebuilds(mdg_ensemble *e, int64_t *rebuilds, int64_t *st
 mdg_status mdg_ensemble_set_graph_mode(mdg_ensemble *e, int use_graphs);
 void *mdg_ensemble_stream(mdg_ensemble *e);
 
+/* ---------------------------------------------------------- executors
+ * An executor the reference's projects run after every MDManager::Calculate()
+ * through MDManager::ExecuteAll, applied here on the device after each step
+ * of mdg_calculate (no host round trip, inside the CUDA graphs):
+ *   GRAVITY  v[axis] += strength * time_step       GravityImposer, src/phaseflow.cc:58-73
+ *   PISTON   wall at z = 0 and a piston at `position` (both the pair-force
+ *            expression at the distance), impulse summed; the position then
+ *            moves by -velocity                    MyPiston, src/rankine.cc:55-97,117-121
+ *   SHELL    spherical wall of radius `radius` around `center`
+ *                                                  ShellForce, src/burst.cc:67-99
+ * time_step is the dt the executor multiplies by (the reference's executors
+ * carry their own). */
+enum {
+  MDG_EXTERNAL_NONE = 0,
+  MDG_EXTERNAL_GRAVITY = 1,
+  MDG_EXTERNAL_PISTON = 2,
+  MDG_EXTERNAL_SHELL = 3
+};
+typedef struct mdg_external {
+  int kind;
+  int axis;
+  double strength;
+  double time_step;
+  double position;
+  double velocity;
+  double center[3];
+  double radius;
+} mdg_external;
+/* NULL or kind NONE turns the executor off. */
+mdg_status mdg_set_external(mdg_handle *h, const mdg_external *x);
+/* Piston position now and impulse of the last pass (MyPiston::position, impulse). */
+mdg_status mdg_external_state(mdg_handle *h, double *position, double *impulse);
+
 /* ---------------------------------------------------------- adjoint
  * Gradients of a trajectory loss, by a reverse sweep over the steps
  * (mdacp_b200/csrc/mdg_adjoint.cu).  No counterpart in the reference, which

@@ -20,6 +20,7 @@ __all__ = [
     "Info",
     "Replica",
     "AdjointParams",
+    "External",
     "System",
     "Ensemble",
     "load_library",
@@ -121,6 +122,24 @@ class AdjointParams(ctypes.Structure):
     ]
 
 
+class External(ctypes.Structure):
+    """Mirror of mdg_external (include/mdacp_b200.h)."""
+
+    _fields_ = [
+        ("kind", ctypes.c_int),
+        ("axis", ctypes.c_int),
+        ("strength", ctypes.c_double),
+        ("time_step", ctypes.c_double),
+        ("position", ctypes.c_double),
+        ("velocity", ctypes.c_double),
+        ("center", ctypes.c_double * 3),
+        ("radius", ctypes.c_double),
+    ]
+
+
+EXTERNAL_NONE, EXTERNAL_GRAVITY, EXTERNAL_PISTON, EXTERNAL_SHELL = 0, 1, 2, 3
+
+
 class Replica(ctypes.Structure):
     """``mdg_replica`` (include/mdacp_b200.h)."""
 
@@ -136,6 +155,8 @@ SIGNATURES = {
     "mdg_adjoint_default_params": (None, [ctypes.POINTER(AdjointParams)]),
     "mdg_adjoint_run": (ctypes.c_int, [ctypes.POINTER(AdjointParams), _DP, _DP, ctypes.c_int, _DP, _DP, _DP, _DP]),
     "mdg_default_params": (None, [ctypes.POINTER(Params)]),
+    "mdg_set_external": (ctypes.c_int, [_H, ctypes.POINTER(External)]),
+    "mdg_external_state": (ctypes.c_int, [_H, _DP, _DP]),
     "mdg_create": (ctypes.c_int, [ctypes.POINTER(Params), ctypes.POINTER(_H)]),
     "mdg_destroy": (ctypes.c_int, [_H]),
     "mdg_set_state": (ctypes.c_int, [_H, _DP, _DP, _IP, ctypes.c_int]),
@@ -407,6 +428,26 @@ class System:
 
     def set_graph_mode(self, use_graphs: bool):
         self._check(self.lib.mdg_set_graph_mode(self.h, int(bool(use_graphs))))
+
+    def set_external(self, kind=EXTERNAL_NONE, axis=0, strength=0.0, time_step=None, position=0.0, velocity=0.0,
+                     center=(0.0, 0.0, 0.0), radius=0.0):
+        """Executor applied on the device after every step (mdg_set_external)."""
+        x = External()
+        x.kind = int(kind)
+        x.axis = int(axis)
+        x.strength = float(strength)
+        x.time_step = float(self.params.time_step if time_step is None else time_step)
+        x.position = float(position)
+        x.velocity = float(velocity)
+        x.center[:] = [float(c) for c in center]
+        x.radius = float(radius)
+        self._check(self.lib.mdg_set_external(self.h, ctypes.byref(x)))
+
+    def external_state(self):
+        """(piston position, impulse of the last pass)."""
+        pos, imp = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mdg_external_state(self.h, ctypes.byref(pos), ctypes.byref(imp)))
+        return pos.value, imp.value
 
     def set_kernel_timing(self, on: bool):
         self._check(self.lib.mdg_set_kernel_timing(self.h, int(bool(on))))

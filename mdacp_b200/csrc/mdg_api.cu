@@ -56,6 +56,7 @@ struct mdg_handle {
   // fused FP32 NVE step: which fixed-point buffer (0: qfix, 1: qfix2) holds
   // every atom's position after the coming step's first half drift; -1: none
   int fix_buf = -1;
+  External ext{};                     // executor applied after every step (kind 0: none)
   std::string err;
 };
 
@@ -202,7 +203,17 @@ void launch_build(mdg_handle *h, cudaStream_t s, int4 *pack = nullptr) {
 // drifts fused, the next step's fixed-point copy packed into the other
 // buffer).
 bool fused_step(const mdg_handle *h) {
-  return h->prm.precision == MDG_FP32_MIXED && h->prm.thermostat == MDG_NVE;
+  return h->prm.precision == MDG_FP32_MIXED && h->prm.thermostat == MDG_NVE && h->ext.kind == 0;
+}
+
+// The executor pass after a step (nothing when none is set); returns kernels.
+int launch_external(mdg_handle *h, cudaStream_t s) {
+  if (h->ext.kind == 0) return 0;
+  const int nb = blocks_for(h->n, kBlock);
+  k_external_begin<<<1, 32, 0, s>>>(h->a);
+  k_external<kBlock><<<nb, kBlock, 0, s>>>(h->a, h->box, h->ext, h->n);
+  k_external_done<<<1, 32, 0, s>>>(h->a, h->ext, nb);
+  return 3;
 }
 
 int4 *fix_buffer(mdg_handle *h, int k) { return k ? h->a.qfix2 : h->a.qfix; }
@@ -300,7 +311,7 @@ int launch_step_tail(mdg_handle *h, cudaStream_t s, cudaEvent_t ev_start, cudaEv
     }
   }
   k_step_done<<<1, 32, 0, s>>>(h->a, h->box);
-  return launches + 1;
+  return launches + 1 + launch_external(h, s);
 }
 
 // ---------------------------------------------------------- graph capture
@@ -521,6 +532,7 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   b.sl = SL;
   b.sl2 = SL * SL;
   b.rc2 = prm->cutoff * prm->cutoff;
+  b.rc = prm->cutoff;
   {  // Variables::Variables, src/variables.cc:21-27
     const double s2 = 1.0 / (prm->cutoff * prm->cutoff);
     const double s6 = s2 * s2 * s2, s8 = s6 * s2, s12 = s6 * s6, s14 = s12 * s2;
@@ -798,6 +810,44 @@ mdg_status mdg_set_control(mdg_handle *h, int thermostat, double aimed_temperatu
     h->fix_buf = -1;
     destroy_graph(h);
   }
+  return MDG_OK;
+}
+
+mdg_status mdg_set_external(mdg_handle *h, const mdg_external *x) {
+  if (!h) return MDG_ERR_INVALID_ARGUMENT;
+  External e{};
+  if (x && x->kind != MDG_EXTERNAL_NONE) {
+    if (x->kind < MDG_EXTERNAL_GRAVITY || x->kind > MDG_EXTERNAL_SHELL || x->axis < 0 || x->axis > 2 ||
+        !std::isfinite(x->time_step) || !std::isfinite(x->strength) || !std::isfinite(x->position) ||
+        !std::isfinite(x->velocity) || !std::isfinite(x->radius))
+      return MDG_ERR_INVALID_ARGUMENT;
+    e.kind = x->kind;
+    e.axis = x->axis;
+    e.strength = x->strength;
+    e.dt = x->time_step;
+    e.velocity = x->velocity;
+    for (int d = 0; d < 3; d++) e.center[d] = x->center[d];
+    e.radius = x->radius;
+  }
+  CUDA_TRY(h, cudaSetDevice(h->prm.device));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  const double pos = x ? x->position : 0.0, zero = 0.0;
+  CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->ext_position, &pos, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->ext_impulse, &zero, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  h->ext = e;
+  h->fix_buf = -1;
+  destroy_graph(h);
+  return MDG_OK;
+}
+
+mdg_status mdg_external_state(mdg_handle *h, double *position, double *impulse) {
+  if (!h) return MDG_ERR_INVALID_ARGUMENT;
+  Status st;
+  mdg_status r = read_status(h, &st);
+  if (r) return r;
+  if (position) *position = st.ext_position;
+  if (impulse) *impulse = st.ext_impulse;
   return MDG_OK;
 }
 

@@ -38,6 +38,7 @@ struct Box {
   double sl;           // SearchLength
   double sl2;          // SearchLength^2
   double rc2;          // CUTOFF_LENGTH^2
+  double rc;           // CUTOFF_LENGTH
   double c0, c2;       // smoothed-LJ constants (Variables::C0, C2)
   double dt;           // TimeStep
   double buffer_length;
@@ -68,6 +69,20 @@ struct Status {
   double zeta;                      // Nose-Hoover friction (Variables::Zeta)
   double sim_time;
   double too_fast_v;                // speed that tripped kErrTooFast
+  double ext_position;              // external executor: current piston position
+  double ext_impulse;               // external executor: impulse of the last pass
+};
+
+// An executor the reference's projects run after every Calculate() (on the
+// real atoms' momenta = velocities), applied on the device after each step.
+struct External {
+  int kind;          // 0 none, 1 gravity, 2 piston, 3 shell wall
+  int axis;          // gravity: axis of the acceleration
+  double strength;   // gravity: acceleration
+  double dt;         // the time step the executor multiplies by
+  double velocity;   // piston: displacement per pass (towards -z)
+  double center[3];  // shell: centre
+  double radius;     // shell: radius of the wall surface
 };
 
 struct Arrays {
@@ -709,6 +724,79 @@ __global__ void __launch_bounds__(BLOCK) k_drift(Arrays a, Box b, int n, int tra
     }
   }
   if (track_vmax) block_max_to<BLOCK>(&a.st->vmax2_bits, v2);
+}
+
+// ------------------------------------------------------------ executors
+// The wall term of the reference's executors: the pair-force expression at
+// distance d, each operation separately rounded (src/rankine.cc:78-82,
+// src/burst.cc:91-93).
+__device__ __forceinline__ double wall_df(double d, double c2, double dt) {
+  const double r2 = dmul(d, d);
+  const double r6 = dmul(dmul(r2, r2), r2);
+  return dmul(dadd(ddiv(dsub(dmul(24.0, r6), 48.0), dmul(dmul(r6, r6), r2)), dmul(c2, 8.0)), dt);
+}
+
+// Before an executor pass: the pass re-takes the |v| maximum the next skin
+// check reads (PairList::IsPairListExpired reads the momenta after it).
+static __global__ void k_external_begin(Arrays a) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && !a.st->error) a.st->vmax2_bits = 0ull;
+}
+
+// One executor pass over all atoms: GravityImposer (src/phaseflow.cc:58-73),
+// MyPiston (src/rankine.cc:55-97), ShellForce (src/burst.cc:67-99); block
+// partial sums of the piston impulse into a.partials.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_external(Arrays a, Box b, External x, int n) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  double v2 = 0.0, imp = 0.0;
+  if (i < n && !a.st->error) {
+    const double4 q = a.q[i];
+    double4 v = a.v[i];
+    const double CL = b.rc;
+    if (x.kind == 1) {
+      const double g = dmul(x.strength, x.dt);
+      if (x.axis == 0) v.x = dadd(v.x, g);
+      else if (x.axis == 1) v.y = dadd(v.y, g);
+      else v.z = dadd(v.z, g);
+    } else if (x.kind == 2) {
+      if (q.z < CL) {
+        const double df = wall_df(q.z, b.c2, x.dt);
+        v.z = dsub(v.z, dmul(df, q.z));
+      }
+      const double pos = a.st->ext_position;
+      if (q.z > pos) {
+        const double dz = dadd(dsub(pos, q.z), CL);
+        const double df = wall_df(dz, b.c2, x.dt);
+        v.z = dadd(v.z, dmul(df, dz));
+        imp = -dmul(df, dz);
+      }
+    } else if (x.kind == 3) {
+      const double dx = dsub(q.x, x.center[0]), dy = dsub(q.y, x.center[1]), dz = dsub(q.z, x.center[2]);
+      const double r = dsub(x.radius, sqrt(dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz))));
+      if (!(dmul(r, r) > b.rc2)) {
+        const double df = wall_df(r, b.c2, x.dt);
+        v.x = dadd(v.x, dmul(df, dx));
+        v.y = dadd(v.y, dmul(df, dy));
+        v.z = dadd(v.z, dmul(df, dz));
+      }
+    }
+    a.v[i] = v;
+    v2 = dadd(dadd(dmul(v.x, v.x), dmul(v.y, v.y)), dmul(v.z, v.z));
+  }
+  block_max_to<BLOCK>(&a.st->vmax2_bits, v2);
+  double s1[1] = {imp};
+  block_sum_to<BLOCK, 1>(s1, a.partials);
+}
+
+// After a pass: impulse (fixed-order sum of the block partials) and the
+// piston's move, as Rankine::Run moves it after each pass
+// (src/rankine.cc:117-121).
+static __global__ void k_external_done(Arrays a, External x, int nblocks) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || a.st->error) return;
+  double s = 0.0;
+  for (int k = 0; k < nblocks; k++) s += a.partials[k];
+  a.st->ext_impulse = s;
+  if (x.kind == 2) a.st->ext_position = dsub(a.st->ext_position, x.velocity);
 }
 
 // Packs q + v dt/2 (the coming step's first half drift) into out without

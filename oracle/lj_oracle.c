@@ -701,6 +701,53 @@ int ljo_step(ljo_system *s, int nsteps) {
   return 0;
 }
 
+/* ------------------------------------------------------------ executors */
+/* The reference's wall term: df of a pair at distance d, the pair force's
+   expression with the separately rounded operations (src/rankine.cc:78-82,
+   src/burst.cc:91-93). */
+static double wall_df(double d, double c2, double dt) {
+  const double r2 = d * d;
+  const double r6 = r2 * r2 * r2;
+  return ((24.0 * r6 - 48.0) / (r6 * r6 * r2) + c2 * 8.0) * dt;
+}
+
+double ljo_apply_external(ljo_system *s, ljo_external *e) {
+  double impulse = 0.0;
+  const double CL = s->prm.rc;
+  if (e->kind == 1) {
+    for (int i = 0; i < s->pn; i++) s->p[i][e->axis] += e->strength * e->time_step;
+  } else if (e->kind == 2) {
+    for (int i = 0; i < s->pn; i++) {
+      if (s->q[i][2] < CL) {
+        const double dz = s->q[i][2];
+        const double df = wall_df(dz, s->c2, e->time_step);
+        s->p[i][2] -= df * dz;
+      }
+      if (s->q[i][2] > e->position) {
+        const double dz = e->position - s->q[i][2] + CL;
+        const double df = wall_df(dz, s->c2, e->time_step);
+        s->p[i][2] += df * dz;
+        impulse -= df * dz;
+      }
+    }
+    e->position -= e->velocity;
+  } else if (e->kind == 3) {
+    const double CL2 = CL * CL;
+    for (int i = 0; i < s->pn; i++) {
+      const double dx = s->q[i][0] - e->center[0];
+      const double dy = s->q[i][1] - e->center[1];
+      const double dz = s->q[i][2] - e->center[2];
+      const double r = e->radius - sqrt(dx * dx + dy * dy + dz * dz);
+      if (r * r > CL2) continue;
+      const double df = wall_df(r, s->c2, e->time_step);
+      s->p[i][0] += df * dx;
+      s->p[i][1] += df * dy;
+      s->p[i][2] += df * dz;
+    }
+  }
+  return impulse;
+}
+
 /* ------------------------------------------------------------ accessors */
 int ljo_particle_number(const ljo_system *s) { return s->pn; }
 int ljo_total_particle_number(const ljo_system *s) { return s->tn; }

@@ -77,6 +77,24 @@ void ljo_forces(ljo_system *s, double *f);
 /* Sums as the observers return them: KE = sum 1/2 p^2, PE, virial = sum(...)/3. */
 void ljo_observe(const ljo_system *s, double *ke, double *pe, double *virial);
 
+/* Executors the reference's projects run after each Calculate() (real atoms,
+   momenta = velocities): kind 1 GravityImposer (src/phaseflow.cc:58-73),
+   2 MyPiston (src/rankine.cc:55-97), 3 ShellForce (src/burst.cc:67-99).
+   Piston: after the pass the position moves by -velocity, as Rankine::Run
+   moves it (src/rankine.cc:117-121); returns the pass's impulse (0 for the
+   other kinds). */
+typedef struct ljo_external {
+  int kind;
+  int axis;          /* gravity */
+  double strength;   /* gravity: acceleration */
+  double time_step;  /* the dt the executor multiplies by */
+  double position;   /* piston */
+  double velocity;   /* piston: displacement per pass */
+  double center[3];  /* shell */
+  double radius;     /* shell: radius of the wall surface */
+} ljo_external;
+double ljo_apply_external(ljo_system *s, ljo_external *e);
+
 /* Philox4x32-10 block (Salmon et al., SC'11), exported for the noise tests. */
 void ljo_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* The three standard normals used for atom `id` at Langevin step `step`. */

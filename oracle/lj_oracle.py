@@ -43,6 +43,22 @@ class Params(ctypes.Structure):
     ]
 
 
+class External(ctypes.Structure):
+    """Mirror of ljo_external: the reference projects' executors (gravity,
+    piston, shell wall), applied after each step."""
+
+    _fields_ = [
+        ("kind", ctypes.c_int),
+        ("axis", ctypes.c_int),
+        ("strength", ctypes.c_double),
+        ("time_step", ctypes.c_double),
+        ("position", ctypes.c_double),
+        ("velocity", ctypes.c_double),
+        ("center", ctypes.c_double * 3),
+        ("radius", ctypes.c_double),
+    ]
+
+
 _lib = None
 
 
@@ -73,6 +89,8 @@ def load_library() -> ctypes.CDLL:
     lib.ljo_observe.argtypes = [ctypes.c_void_p, dp, dp, dp]
     lib.ljo_philox4x32.argtypes = [P(ctypes.c_uint32), P(ctypes.c_uint32), P(ctypes.c_uint32)]
     lib.ljo_langevin_normals.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, dp]
+    lib.ljo_apply_external.argtypes = [ctypes.c_void_p, P(External)]
+    lib.ljo_apply_external.restype = ctypes.c_double
     _lib = lib
     return lib
 
@@ -122,6 +140,10 @@ class Oracle:
     def step(self, n):
         if self.lib.ljo_step(self.h, n) != 0:
             raise RuntimeError("oracle: step failed (too fast particle or invalid position)")
+
+    def apply_external(self, ext: "External") -> float:
+        """One executor pass (ljo_apply_external); returns the impulse."""
+        return self.lib.ljo_apply_external(self.h, ctypes.byref(ext))
 
     @property
     def n(self):
