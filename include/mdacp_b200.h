@@ -42,7 +42,8 @@ enum {
   MDG_ERR_BOX_TOO_SMALL = -7,    /* fewer than 3 cells along an axis */
   MDG_ERR_TIMEOUT = -8,          /* a bounded device wait gave up */
   MDG_ERR_STATE = -9,            /* call out of order (e.g. no state uploaded) */
-  MDG_ERR_NO_DEVICE = -10
+  MDG_ERR_NO_DEVICE = -10,
+  MDG_ERR_IO = -11               /* a file could not be read or written, or is not a checkpoint */
 };
 
 enum { MDG_FP64 = 0, MDG_FP32_MIXED = 1 };
@@ -242,6 +243,28 @@ mdg_status mdg_ensemble_observe(mdg_ensemble *e, double *ke, double *pe, double 
 mdg_status mdg_ensemble_rebuilds(mdg_ensemble *e, int64_t *rebuilds, int64_t *steps);
 mdg_status mdg_ensemble_set_graph_mode(mdg_ensemble *e, int use_graphs);
 void *mdg_ensemble_stream(mdg_ensemble *e);
+
+/* ---------------------------------------------------------- checkpoints and snapshots
+ * A checkpoint holds the handle's whole state: atoms in slot order with their
+ * ids and types, positions at the last list build, the skin budget, step and
+ * build counters, simulation time, zeta and the executor's state.  A handle
+ * created with the same parameters and loaded from it continues bit for bit
+ * as the saved handle would have (the list is rebuilt from the positions of
+ * the last build).  The reference's Variables::SaveToStream and
+ * LoadFromStream (src/variables.cc:115-136) are not symmetric: the reader
+ * expects a header the writer never writes; this format has one. */
+mdg_status mdg_save_checkpoint(mdg_handle *h, const char *path);
+mdg_status mdg_load_checkpoint(mdg_handle *h, const char *path);
+/* The reference's text snapshots, from the device state: CDVIEW as
+ * MDUnit::SaveAsCdview ("0 type x y z px py pz", src/mdunit.cc:67-83),
+ * CONFIGURATION as Variables::SaveConfiguration ("x y z px py pz",
+ * src/variables.cc:49-61).  The device-to-host copy is queued on the
+ * handle's stream and a host thread writes the file, so the caller can keep
+ * queuing steps; mdg_snapshot_wait joins every pending writer and reports
+ * the first failure. */
+enum { MDG_SNAPSHOT_CDVIEW = 0, MDG_SNAPSHOT_CONFIGURATION = 1 };
+mdg_status mdg_snapshot_async(mdg_handle *h, const char *path, int format);
+mdg_status mdg_snapshot_wait(mdg_handle *h);
 
 /* ---------------------------------------------------------- executors
  * An executor the reference's projects run after every MDManager::Calculate()

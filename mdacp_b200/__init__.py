@@ -49,6 +49,7 @@ STATUS_NAMES = {
     -8: "MDG_ERR_TIMEOUT",
     -9: "MDG_ERR_STATE",
     -10: "MDG_ERR_NO_DEVICE",
+    -11: "MDG_ERR_IO",
 }
 
 
@@ -138,6 +139,7 @@ class External(ctypes.Structure):
 
 
 EXTERNAL_NONE, EXTERNAL_GRAVITY, EXTERNAL_PISTON, EXTERNAL_SHELL = 0, 1, 2, 3
+SNAPSHOT_CDVIEW, SNAPSHOT_CONFIGURATION = 0, 1
 
 
 class Replica(ctypes.Structure):
@@ -156,6 +158,10 @@ SIGNATURES = {
     "mdg_adjoint_run": (ctypes.c_int, [ctypes.POINTER(AdjointParams), _DP, _DP, ctypes.c_int, _DP, _DP, _DP, _DP]),
     "mdg_default_params": (None, [ctypes.POINTER(Params)]),
     "mdg_set_external": (ctypes.c_int, [_H, ctypes.POINTER(External)]),
+    "mdg_save_checkpoint": (ctypes.c_int, [_H, ctypes.c_char_p]),
+    "mdg_load_checkpoint": (ctypes.c_int, [_H, ctypes.c_char_p]),
+    "mdg_snapshot_async": (ctypes.c_int, [_H, ctypes.c_char_p, ctypes.c_int]),
+    "mdg_snapshot_wait": (ctypes.c_int, [_H]),
     "mdg_external_state": (ctypes.c_int, [_H, _DP, _DP]),
     "mdg_create": (ctypes.c_int, [ctypes.POINTER(Params), ctypes.POINTER(_H)]),
     "mdg_destroy": (ctypes.c_int, [_H]),
@@ -428,6 +434,25 @@ class System:
 
     def set_graph_mode(self, use_graphs: bool):
         self._check(self.lib.mdg_set_graph_mode(self.h, int(bool(use_graphs))))
+
+    def save_checkpoint(self, path):
+        """Whole state to a file (mdg_save_checkpoint)."""
+        self._check(self.lib.mdg_save_checkpoint(self.h, str(path).encode()))
+
+    def load_checkpoint(self, path):
+        """Restore a checkpoint into this handle (same box and parameters);
+        the trajectory continues bit for bit."""
+        self._check(self.lib.mdg_load_checkpoint(self.h, str(path).encode()))
+        n = ctypes.c_int()
+        self._check(self.lib.mdg_particle_number(self.h, ctypes.byref(n)))
+        self.n = n.value
+
+    def snapshot_async(self, path, fmt=0):
+        """Queue a text snapshot (0: .cd cdview lines, 1: .cnf configuration)."""
+        self._check(self.lib.mdg_snapshot_async(self.h, str(path).encode(), int(fmt)))
+
+    def snapshot_wait(self):
+        self._check(self.lib.mdg_snapshot_wait(self.h))
 
     def set_external(self, kind=EXTERNAL_NONE, axis=0, strength=0.0, time_step=None, position=0.0, velocity=0.0,
                      center=(0.0, 0.0, 0.0), radius=0.0):

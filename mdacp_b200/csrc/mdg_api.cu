@@ -7,7 +7,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
+#include <fstream>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "mdacp_b200.h"
@@ -57,6 +61,9 @@ struct mdg_handle {
   // every atom's position after the coming step's first half drift; -1: none
   int fix_buf = -1;
   External ext{};                     // executor applied after every step (kind 0: none)
+  std::vector<std::thread> writers;   // pending snapshot writers
+  std::mutex writer_mutex;
+  std::string writer_error;           // first failure of a writer
   std::string err;
 };
 
@@ -614,6 +621,7 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
 
 mdg_status mdg_destroy(mdg_handle *h) {
   if (!h) return MDG_ERR_INVALID_ARGUMENT;
+  for (auto &t : h->writers) t.join();
   cudaSetDevice(h->prm.device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   destroy_graph(h);
@@ -1104,10 +1112,230 @@ const char *mdg_status_string(mdg_status s) {
     case MDG_ERR_TIMEOUT: return "device wait timed out";
     case MDG_ERR_STATE: return "call out of order";
     case MDG_ERR_NO_DEVICE: return "no CUDA device";
+    case MDG_ERR_IO: return "file error";
   }
   return "unknown status";
 }
 
 const char *mdg_version(void) { return "mdacp_b200 0.1 (sm_100a)"; }
+
+// ------------------------------------------------------ checkpoints
+namespace {
+struct CkptHeader {
+  char magic[8];
+  int version;
+  int n;
+  double L[3];
+  double cutoff, buffer_length, time_step;
+  int precision, thermostat;
+  double aimed_temperature, heatbath_tau, heatbath_gamma;
+  uint64_t seed;
+  int check_list_length;
+  int observer_mode;
+  double obs_lag;
+  Status st;
+  External ext;
+};
+const char kCkptMagic[8] = {'M', 'D', 'G', 'C', 'K', 'P', 'T', '1'};
+}  // namespace
+
+mdg_status mdg_save_checkpoint(mdg_handle *h, const char *path) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (!path) return MDG_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(h, cudaSetDevice(h->prm.device));
+  CkptHeader hd{};
+  memcpy(hd.magic, kCkptMagic, 8);
+  hd.version = 1;
+  hd.n = h->n;
+  for (int d = 0; d < 3; d++) hd.L[d] = h->prm.L[d];
+  hd.cutoff = h->prm.cutoff;
+  hd.buffer_length = h->prm.buffer_length;
+  hd.time_step = h->prm.time_step;
+  hd.precision = h->prm.precision;
+  hd.thermostat = h->prm.thermostat;
+  hd.aimed_temperature = h->prm.aimed_temperature;
+  hd.heatbath_tau = h->prm.heatbath_tau;
+  hd.heatbath_gamma = h->prm.heatbath_gamma;
+  hd.seed = h->prm.seed;
+  hd.check_list_length = h->prm.check_list_length;
+  hd.observer_mode = h->observer_mode;
+  hd.obs_lag = h->obs_lag;
+  hd.ext = h->ext;
+  if ((r = read_status(h, &hd.st))) return r;
+  if (hd.st.error) return translate_device_error(h, hd.st);
+  const int n = h->n;
+  std::vector<double4> q(n), v(n), qo(n);
+  std::vector<int> ids(n), ty(n);
+  if (n > 0) {
+    CUDA_TRY(h, cudaMemcpyAsync(q.data(), h->a.q, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(v.data(), h->a.v, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(qo.data(), h->a.q_old, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(ids.data(), h->a.ids, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(ty.data(), h->a.type, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  }
+  std::ofstream f(path, std::ios::binary | std::ios::trunc);
+  if (!f) return fail(h, MDG_ERR_IO, std::string("cannot write ") + path);
+  f.write((const char *)&hd, sizeof hd);
+  f.write((const char *)q.data(), sizeof(double4) * n);
+  f.write((const char *)v.data(), sizeof(double4) * n);
+  f.write((const char *)qo.data(), sizeof(double4) * n);
+  f.write((const char *)ids.data(), sizeof(int) * n);
+  f.write((const char *)ty.data(), sizeof(int) * n);
+  if (!f) return fail(h, MDG_ERR_IO, std::string("write failed: ") + path);
+  return MDG_OK;
+}
+
+mdg_status mdg_load_checkpoint(mdg_handle *h, const char *path) {
+  if (!h || !path) return MDG_ERR_INVALID_ARGUMENT;
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return fail(h, MDG_ERR_IO, std::string("cannot read ") + path);
+  CkptHeader hd{};
+  f.read((char *)&hd, sizeof hd);
+  if (!f || memcmp(hd.magic, kCkptMagic, 8) != 0 || hd.version != 1 || hd.n < 0)
+    return fail(h, MDG_ERR_IO, std::string("not a checkpoint of this library: ") + path);
+  for (int d = 0; d < 3; d++)
+    if (hd.L[d] != h->prm.L[d]) return fail(h, MDG_ERR_INVALID_ARGUMENT, "checkpoint box differs from the handle's");
+  if (hd.cutoff != h->prm.cutoff || hd.buffer_length != h->prm.buffer_length || hd.time_step != h->prm.time_step ||
+      hd.precision != h->prm.precision || hd.seed != h->prm.seed ||
+      hd.check_list_length != h->prm.check_list_length)
+    return fail(h, MDG_ERR_INVALID_ARGUMENT, "checkpoint parameters differ from the handle's");
+  const int n = hd.n;
+  if (n > h->cap) return fail(h, MDG_ERR_CAPACITY, "checkpoint holds more atoms than the handle's capacity");
+  std::vector<double4> q(n), v(n), qo(n);
+  std::vector<int> ids(n), ty(n);
+  f.read((char *)q.data(), sizeof(double4) * n);
+  f.read((char *)v.data(), sizeof(double4) * n);
+  f.read((char *)qo.data(), sizeof(double4) * n);
+  f.read((char *)ids.data(), sizeof(int) * n);
+  f.read((char *)ty.data(), sizeof(int) * n);
+  if (!f) return fail(h, MDG_ERR_IO, std::string("truncated checkpoint: ") + path);
+  mdg_status r = mdg_set_control(h, hd.thermostat, hd.aimed_temperature, hd.heatbath_tau, hd.heatbath_gamma);
+  if (r) return r;
+  CUDA_TRY(h, cudaSetDevice(h->prm.device));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  const bool stale = hd.st.list_stale != 0;
+  if (n > 0) {
+    // the list is rebuilt from the positions of the last build: slots come
+    // back in the same order and the rows entry for entry
+    if (h->prm.max_neighbors <= 0) {
+      std::vector<double> q4((size_t)4 * n);
+      for (int i = 0; i < n; i++) {
+        const double4 &x = stale ? q[i] : qo[i];
+        q4[4 * i] = x.x;
+        q4[4 * i + 1] = x.y;
+        q4[4 * i + 2] = x.z;
+        q4[4 * i + 3] = 0.0;
+      }
+      if ((r = alloc_neighbors(h, estimate_max_neighbors(h, q4.data(), n)))) return r;
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.q, stale ? q.data() : qo.data(), sizeof(double4) * n, cudaMemcpyHostToDevice,
+                                h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.v, v.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.ids, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.type, ty.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+  }
+  Status st = hd.st;
+  st.error = 0;
+  st.list_stale = 1;
+  CUDA_TRY(h, cudaMemcpyAsync(h->a.st, &st, sizeof(Status), cudaMemcpyHostToDevice, h->stream));
+  if (n != h->n) h->graph_dirty = true;
+  h->n = n;
+  h->state_set = true;
+  h->fix_buf = -1;
+  destroy_graph(h);
+  if (n > 0 && !stale) {
+    if ((r = ensure_list(h))) return r;
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.q, q.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.v, v.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
+    Status built;
+    if ((r = read_status(h, &built))) return r;
+    st = hd.st;  // counters, budget, clocks as saved; list figures from the rebuild
+    st.max_row = built.max_row;
+    st.list_entries = built.list_entries;
+    st.total_images = built.total_images;
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.st, &st, sizeof(Status), cudaMemcpyHostToDevice, h->stream));
+  } else {
+    st = hd.st;
+    st.list_stale = 1;
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.st, &st, sizeof(Status), cudaMemcpyHostToDevice, h->stream));
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  h->ext = hd.ext;
+  h->observer_mode = hd.observer_mode;
+  h->obs_lag = hd.obs_lag;
+  return MDG_OK;
+}
+
+// ------------------------------------------------------ snapshots
+mdg_status mdg_snapshot_async(mdg_handle *h, const char *path, int format) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (!path || (format != MDG_SNAPSHOT_CDVIEW && format != MDG_SNAPSHOT_CONFIGURATION))
+    return MDG_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(h, cudaSetDevice(h->prm.device));
+  const int n = h->n;
+  double4 *hq = nullptr, *hv = nullptr;
+  int *ht = nullptr;
+  CUDA_TRY(h, cudaHostAlloc((void **)&hq, sizeof(double4) * std::max(n, 1), cudaHostAllocDefault));
+  cudaError_t e = cudaHostAlloc((void **)&hv, sizeof(double4) * std::max(n, 1), cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaHostAlloc((void **)&ht, sizeof(int) * std::max(n, 1), cudaHostAllocDefault);
+  cudaEvent_t done = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(hq, h->a.q, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(hv, h->a.v, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(ht, h->a.type, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(done, h->stream);
+  if (e != cudaSuccess) {
+    if (done) cudaEventDestroy(done);
+    cudaFreeHost(hq);
+    if (hv) cudaFreeHost(hv);
+    if (ht) cudaFreeHost(ht);
+    return fail(h, MDG_ERR_CUDA, std::string("snapshot copy: ") + cudaGetErrorString(e));
+  }
+  const std::string file(path);
+  const int dev = h->prm.device;
+  h->writers.emplace_back([h, file, format, n, hq, hv, ht, done, dev]() {
+    cudaSetDevice(dev);
+    const cudaError_t ce = cudaEventSynchronize(done);
+    bool ok = ce == cudaSuccess;
+    if (ok) {
+      FILE *fp = fopen(file.c_str(), "w");
+      ok = fp != nullptr;
+      for (int i = 0; ok && i < n; i++) {
+        // the reference streams doubles with the default ostream format (%g)
+        if (format == MDG_SNAPSHOT_CDVIEW)
+          ok = fprintf(fp, "0 %d %g %g %g %g %g %g\n", ht[i], hq[i].x, hq[i].y, hq[i].z, hv[i].x, hv[i].y,
+                       hv[i].z) > 0;
+        else
+          ok = fprintf(fp, "%g %g %g %g %g %g\n", hq[i].x, hq[i].y, hq[i].z, hv[i].x, hv[i].y, hv[i].z) > 0;
+      }
+      if (fp && fclose(fp) != 0) ok = false;
+    }
+    cudaEventDestroy(done);
+    cudaFreeHost(hq);
+    cudaFreeHost(hv);
+    cudaFreeHost(ht);
+    if (!ok) {
+      std::lock_guard<std::mutex> lock(h->writer_mutex);
+      if (h->writer_error.empty()) h->writer_error = "snapshot not written: " + file;
+    }
+  });
+  return MDG_OK;
+}
+
+mdg_status mdg_snapshot_wait(mdg_handle *h) {
+  if (!h) return MDG_ERR_INVALID_ARGUMENT;
+  for (auto &t : h->writers) t.join();
+  h->writers.clear();
+  std::lock_guard<std::mutex> lock(h->writer_mutex);
+  if (!h->writer_error.empty()) {
+    const std::string msg = h->writer_error;
+    h->writer_error.clear();
+    return fail(h, MDG_ERR_IO, msg);
+  }
+  return MDG_OK;
+}
 
 }  // extern "C"
