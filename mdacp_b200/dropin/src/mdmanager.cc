@@ -74,6 +74,16 @@ void MDManager::SaveAsCdviewSequential(void) {
 }
 
 void MDManager::SaveAsCdview(const char *filename) {
+  // one unit (the GPU domain): the device copies its state on the stream and
+  // a host thread writes the file (mdg_snapshot_async), so the steps queued
+  // after this call are not held up by the file write
+  if (mdv.size() == 1 && mdv[0]->Vars()->Device()) {
+    Variables *vars = mdv[0]->Vars();
+    vars->SyncToDevice();
+    mdg_check(vars->Device(), mdg_snapshot_async(vars->Device(), filename, MDG_SNAPSHOT_CDVIEW),
+              "mdg_snapshot_async");
+    return;
+  }
   std::ofstream ofs(filename);
   for (size_t i = 0; i < mdv.size(); i++) mdv[i]->SaveAsCdview(ofs);
 }

@@ -62,3 +62,18 @@ def test_dropin_fixtures_present():
     for name in CASES:
         assert (GOLDEN / f"dropin_{name}.cfg").exists()
         assert observe_rows((GOLDEN / f"dropin_{name}.ref.txt").read_text()).shape[0] >= 5
+
+
+@pytest.mark.gpu
+def test_cdview_snapshots_written_from_the_device(tmp_path):
+    # Collision saves conf%04d.cd snapshots through MDManager::SaveAsCdview,
+    # which the drop-in hands to the device's asynchronous writer
+    run_dropin("collision_rc30", tmp_path)
+    files = sorted(tmp_path.glob("conf*.cd"))
+    assert files
+    for f in files:
+        rows = np.loadtxt(f, ndmin=2)
+        assert rows.shape[1] == 8 and rows.shape[0] > 0
+        assert np.all(rows[:, 0] == 0)
+        assert np.all(np.isfinite(rows))
+    assert len({np.loadtxt(f, ndmin=2).shape[0] for f in files}) == 1
