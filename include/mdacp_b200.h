@@ -244,6 +244,20 @@ mdg_status mdg_ensemble_rebuilds(mdg_ensemble *e, int64_t *rebuilds, int64_t *st
 mdg_status mdg_ensemble_set_graph_mode(mdg_ensemble *e, int use_graphs);
 void *mdg_ensemble_stream(mdg_ensemble *e);
 
+/* ---------------------------------------------------------- box and grid analysis
+ * MDManager::ChangeScale (src/mdmanager.cc:573-585) on the device: the list
+ * is built (atoms wrapped into the box), the box and every position are
+ * scaled by alpha, the cell grid is recomputed and the list rebuilt. */
+mdg_status mdg_change_scale(mdg_handle *h, double alpha);
+/* Atoms per cell of a regular grid, as BubbleHist::Analyse counts them
+ * (src/cavitation.cc:38-58, 117-146): dims[d] = int(L_d / grid_size + 0.5)
+ * cells per axis with one edge L_x / dims[0], x fastest, counts as unsigned
+ * char (wrapping at 256 like the reference's counters), positions wrapped
+ * into the box.  out needs dims[0]*dims[1]*dims[2] bytes (cap).  Unlike
+ * BubbleHist::Analyse it does not rebuild the pairlist; call
+ * mdg_make_pairlist first for the reference's rebuild schedule. */
+mdg_status mdg_density_grid(mdg_handle *h, double grid_size, unsigned char *out, int64_t cap, int dims[3]);
+
 /* ---------------------------------------------------------- checkpoints and snapshots
  * A checkpoint holds the handle's whole state: atoms in slot order with their
  * ids and types, positions at the last list build, the skin budget, step and

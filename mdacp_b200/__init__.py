@@ -158,6 +158,8 @@ SIGNATURES = {
     "mdg_adjoint_run": (ctypes.c_int, [ctypes.POINTER(AdjointParams), _DP, _DP, ctypes.c_int, _DP, _DP, _DP, _DP]),
     "mdg_default_params": (None, [ctypes.POINTER(Params)]),
     "mdg_set_external": (ctypes.c_int, [_H, ctypes.POINTER(External)]),
+    "mdg_change_scale": (ctypes.c_int, [_H, ctypes.c_double]),
+    "mdg_density_grid": (ctypes.c_int, [_H, ctypes.c_double, ctypes.POINTER(ctypes.c_ubyte), ctypes.c_int64, _IP]),
     "mdg_save_checkpoint": (ctypes.c_int, [_H, ctypes.c_char_p]),
     "mdg_load_checkpoint": (ctypes.c_int, [_H, ctypes.c_char_p]),
     "mdg_snapshot_async": (ctypes.c_int, [_H, ctypes.c_char_p, ctypes.c_int]),
@@ -434,6 +436,20 @@ class System:
 
     def set_graph_mode(self, use_graphs: bool):
         self._check(self.lib.mdg_set_graph_mode(self.h, int(bool(use_graphs))))
+
+    def change_scale(self, alpha):
+        """MDManager::ChangeScale on the device (box and positions times alpha)."""
+        self._check(self.lib.mdg_change_scale(self.h, float(alpha)))
+        self.params.L[:] = [x * float(alpha) for x in self.params.L]
+
+    def density_grid(self, grid_size):
+        """Atoms per cell of BubbleHist's grid, uint8 array (nz, ny, nx)."""
+        dims = (ctypes.c_int * 3)()
+        g = [int(x / grid_size + 0.5) for x in self.params.L]
+        out = np.zeros(g[0] * g[1] * g[2], dtype=np.uint8)
+        self._check(self.lib.mdg_density_grid(self.h, float(grid_size),
+                                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), out.size, dims))
+        return out.reshape(dims[2], dims[1], dims[0])
 
     def save_checkpoint(self, path):
         """Whole state to a file (mdg_save_checkpoint)."""

@@ -28,6 +28,26 @@ constexpr int kStepsPerGraph = 20;
 
 int blocks_for(int n, int b) { return n > 0 ? (n + b - 1) / b : 1; }
 
+// The box-dependent part of the geometry: MeshList::ChangeScale's cell grid
+// int(L / SL) per axis (src/meshlist.cc:50-52), cell edges, the minimum-image
+// half box and the fixed-point unit.  False when an axis has < 3 cells.
+bool box_geometry(mdg::Box &b, const double L[3], double SL) {
+  for (int d = 0; d < 3; d++) {
+    const int ms = (int)(L[d] / SL);
+    if (ms < 3) return false;
+  }
+  for (int d = 0; d < 3; d++) {
+    b.L[d] = L[d];
+    b.hL[d] = 0.5 * L[d];
+    b.ms[d] = (int)(L[d] / SL);
+    b.inv_cs[d] = (double)b.ms[d] / L[d];
+    b.fix_scale[d] = (float)(L[d] / 4294967296.0);
+    b.cs[d] = L[d] / (double)b.ms[d];
+  }
+  b.ncell = b.ms[0] * b.ms[1] * b.ms[2];
+  return true;
+}
+
 }  // namespace
 
 struct mdg_handle {
@@ -60,6 +80,7 @@ struct mdg_handle {
   // fused FP32 NVE step: which fixed-point buffer (0: qfix, 1: qfix2) holds
   // every atom's position after the coming step's first half drift; -1: none
   int fix_buf = -1;
+  int cell_cap = 0;                   // cells the cell tables hold
   External ext{};                     // executor applied after every step (kind 0: none)
   std::vector<std::thread> writers;   // pending snapshot writers
   std::mutex writer_mutex;
@@ -524,18 +545,10 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   h->prm = *prm;
   Box &b = h->box;
   const double SL = prm->cutoff + prm->buffer_length;  // src/simulationinfo.cc:6-7
-  for (int d = 0; d < 3; d++) {
-    b.L[d] = prm->L[d];
-    b.hL[d] = 0.5 * prm->L[d];
-    b.ms[d] = (int)(prm->L[d] / SL);  // MeshList::ChangeScale, src/meshlist.cc:50-52
-    if (b.ms[d] < 3) {
-      delete h;
-      return MDG_ERR_BOX_TOO_SMALL;
-    }
-    b.inv_cs[d] = (double)b.ms[d] / prm->L[d];
-    b.fix_scale[d] = (float)(prm->L[d] / 4294967296.0);
+  if (!box_geometry(b, prm->L, SL)) {
+    delete h;
+    return MDG_ERR_BOX_TOO_SMALL;
   }
-  b.ncell = b.ms[0] * b.ms[1] * b.ms[2];
   b.sl = SL;
   b.sl2 = SL * SL;
   b.rc2 = prm->cutoff * prm->cutoff;
@@ -551,11 +564,11 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   b.rc2f = (float)b.rc2;
   b.c2x8f = (float)(b.c2 * 8.0);
   b.check_list_length = prm->check_list_length;
-  for (int d = 0; d < 3; d++) b.cs[d] = prm->L[d] / (double)b.ms[d];
   // FP32 prefilter band: FP32 r^2 within 1e-4 SL^2 of SL^2 is decided in FP64
   b.sl2_lo = (float)(b.sl2 * (1.0 - 1e-4));
   b.sl2_hi = (float)(b.sl2 * (1.0 + 1e-4));
   h->ncell = b.ncell;
+  h->cell_cap = b.ncell;
   h->cap = prm->capacity;
 
   cudaError_t e = cudaSetDevice(prm->device);
@@ -846,6 +859,75 @@ mdg_status mdg_set_external(mdg_handle *h, const mdg_external *x) {
   h->ext = e;
   h->fix_buf = -1;
   destroy_graph(h);
+  return MDG_OK;
+}
+
+mdg_status mdg_change_scale(mdg_handle *h, double alpha) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (!(alpha > 0.0) || !std::isfinite(alpha)) return MDG_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(h, cudaSetDevice(h->prm.device));
+  double L[3];
+  for (int d = 0; d < 3; d++) L[d] = h->prm.L[d] * alpha;  // MDManager::ChangeScale, src/mdmanager.cc:573-585
+  Box nb = h->box;
+  if (!box_geometry(nb, L, h->box.sl)) return fail(h, MDG_ERR_BOX_TOO_SMALL, "scaled box below 3 cells per axis");
+  // the reference builds the list (wrapping the atoms into the box) before
+  // scaling and again after it
+  const int one = 1;
+  CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->list_stale, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  if ((r = ensure_list(h))) return r;
+  if (h->n > 0)
+    k_scale_positions<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->n, alpha);
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (nb.ncell > h->cell_cap) {
+    cudaFree(h->a.cell_count);
+    cudaFree(h->a.cell_start);
+    cudaFree(h->d_tiles);
+    h->a.cell_count = h->a.cell_start = h->d_tiles = nullptr;
+    CUDA_TRY(h, dalloc(&h->a.cell_count, nb.ncell));
+    CUDA_TRY(h, dalloc(&h->a.cell_start, nb.ncell + 1));
+    CUDA_TRY(h, dalloc(&h->d_tiles, (size_t)blocks_for(nb.ncell, kScanBlock) + 1));
+    h->cell_cap = nb.ncell;
+  }
+  h->box = nb;
+  h->ncell = nb.ncell;
+  for (int d = 0; d < 3; d++) h->prm.L[d] = L[d];
+  h->fix_buf = -1;
+  destroy_graph(h);
+  CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->list_stale, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  return ensure_list(h);
+}
+
+mdg_status mdg_density_grid(mdg_handle *h, double grid_size, unsigned char *out, int64_t cap, int dims[3]) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (!(grid_size > 0.0) || !dims || cap < 0) return MDG_ERR_INVALID_ARGUMENT;
+  // BubbleHist (src/cavitation.cc:38-58): grid counts int(w / g + 0.5) per
+  // axis, one grid edge from the x width
+  int g[3];
+  for (int d = 0; d < 3; d++) {
+    g[d] = (int)(h->prm.L[d] / grid_size + 0.5);
+    if (g[d] < 1) return MDG_ERR_INVALID_ARGUMENT;
+    dims[d] = g[d];
+  }
+  const int64_t cells = (int64_t)g[0] * g[1] * g[2];
+  if (!out || cap < cells) return cells <= cap ? MDG_ERR_INVALID_ARGUMENT : fail(h, MDG_ERR_CAPACITY, "grid larger than cap");
+  const double gs = h->prm.L[0] / (double)g[0];
+  CUDA_TRY(h, cudaSetDevice(h->prm.device));
+  int *count = nullptr;
+  CUDA_TRY(h, dalloc(&count, (size_t)cells));
+  cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int) * cells, h->stream);
+  if (e == cudaSuccess && h->n > 0)
+    k_density<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n, 1.0 / gs, g[0], g[1],
+                                                                          g[2], count);
+  std::vector<int> hc((size_t)cells);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hc.data(), count, sizeof(int) * cells, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(count);
+  if (e != cudaSuccess) return fail(h, MDG_ERR_CUDA, std::string("density grid: ") + cudaGetErrorString(e));
+  for (int64_t k = 0; k < cells; k++) out[k] = (unsigned char)(hc[(size_t)k] & 255);
   return MDG_OK;
 }
 

@@ -799,6 +799,38 @@ static __global__ void k_external_done(Arrays a, External x, int nblocks) {
   if (x.kind == 2) a.st->ext_position = dsub(a.st->ext_position, x.velocity);
 }
 
+// Variables::ChangeScale (src/variables.cc:141-148): q *= alpha.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scale_positions(Arrays a, int n, double alpha) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= n) return;
+  double4 q = a.q[i];
+  q.x = dmul(q.x, alpha);
+  q.y = dmul(q.y, alpha);
+  q.z = dmul(q.z, alpha);
+  a.q[i] = q;
+}
+
+// Atoms per cell of a regular grid (BubbleHist::AnalyseSub,
+// src/cavitation.cc:117-146): index int((x - 0) / grid_size) per axis on the
+// wrapped position, x fastest; counts kept in int, cast to unsigned char by
+// the caller as the reference's counters wrap.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_density(Arrays a, Box b, int n, double gsinv, int gx, int gy, int gz,
+                                                   int *count) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= n) return;
+  const double4 q = a.q[i];
+  double x[3] = {q.x, q.y, q.z};
+  int g[3] = {gx, gy, gz}, c[3];
+  for (int d = 0; d < 3; d++) {
+    x[d] -= b.L[d] * floor(x[d] / b.L[d]);
+    const int k = (int)(x[d] * gsinv);
+    c[d] = k < 0 ? 0 : (k >= g[d] ? g[d] - 1 : k);
+  }
+  atomicAdd(&count[c[0] + c[1] * gx + c[2] * gx * gy], 1);
+}
+
 // Packs q + v dt/2 (the coming step's first half drift) into out without
 // moving atoms: the fixed-point copy the fused NVE force pass reads.
 template <int BLOCK>

@@ -129,15 +129,11 @@ void MDUnit::MakePairList(void) {
 }
 
 void MDUnit::ChangeScale(double alpha) {
-  vars->SyncToHost();
+  // the device scales its box and positions and rebuilds its cell grid
+  // (mdg_change_scale); the host mirror follows on its next download
+  vars->SyncToDevice();
   myrect.ChangeScale(alpha);
-  vars->ChangeScale(alpha);
   mesh->ChangeScale(sinfo, myrect);
-  // the box is part of the device handle: rebuild it with the new lengths
-  const double zeta = vars->Zeta;
-  mdg_destroy(dev);
-  dev = nullptr;
-  CreateDevice();
-  vars->Zeta = zeta;
-  vars->MarkHostDirty();
+  mdg_check(dev, mdg_change_scale(dev, alpha), "mdg_change_scale");
+  vars->MarkDeviceNewer();
 }

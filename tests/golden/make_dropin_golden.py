@@ -29,6 +29,12 @@ CASES = {
                                        "AimedTemperature": "1.5", "HeatbathTau": "0.1"}),
     "collision_rc30": (3.0, {"Mode": "Collision", "SystemSize": "40", "TimeStep": "0.005",
                              "TotalLoop": "300", "ObserveLoop": "50"}),
+    # thermalise (Nose-Hoover), ChangeScale 1.05, then bubble histograms
+    # (conf%04d.dat, one byte per grid cell) every ObserveLoop steps
+    "cavitation_rc25": (2.5, {"Mode": "Cavitation", "Density": "0.7", "SystemSize": "12",
+                              "TimeStep": "0.005", "ThermalizeLoop": "100", "TotalLoop": "200",
+                              "ObserveLoop": "50", "InitialVelocity": "1.0", "AimedTemperature": "0.9",
+                              "ChangeScale": "1.05", "GridSize": "3.0"}),
 }
 
 
@@ -44,6 +50,8 @@ def main():
             (pathlib.Path(wd) / "input.cfg").write_text(cfg_text(lines))
             out = subprocess.run([str(binary), "-i", "input.cfg"], cwd=wd, capture_output=True, text=True,
                                  env=dict(os.environ, OMP_NUM_THREADS="1"), check=True)
+            for dat in sorted(pathlib.Path(wd).glob("conf*.dat")):  # bubble histograms
+                (OUT / f"dropin_{name}.{dat.name}").write_bytes(dat.read_bytes())
         (OUT / f"dropin_{name}.cfg").write_text(cfg_text(lines))
         (OUT / f"dropin_{name}.ref.txt").write_text(out.stdout)
         print(name, len(out.stdout.splitlines()), "lines")

@@ -77,3 +77,39 @@ def test_cdview_snapshots_written_from_the_device(tmp_path):
         assert np.all(rows[:, 0] == 0)
         assert np.all(np.isfinite(rows))
     assert len({np.loadtxt(f, ndmin=2).shape[0] for f in files}) == 1
+
+
+def labelled_rows(text, label):
+    """Numeric columns of the lines ending in `# label`, without the last
+    column (the run's wall-clock time)."""
+    rows = []
+    for line in text.splitlines():
+        if line.rstrip().endswith("# " + label):
+            rows.append([float(x) for x in line.split("#")[0].split()][:-1])
+    return np.array(rows)
+
+
+@pytest.mark.gpu
+def test_cavitation_change_scale_and_bubble_histograms(tmp_path):
+    # Cavitation: Nose-Hoover thermalisation, MDManager::ChangeScale (on the
+    # device), then BubbleHist density grids (conf%04d.dat) every 50 steps
+    binary = BUILD / "mdacp_rc25"
+    if not binary.exists():
+        pytest.skip(f"{binary} not built")
+    (tmp_path / "input.cfg").write_text((GOLDEN / "dropin_cavitation_rc25.cfg").read_text())
+    out = subprocess.run([str(binary), "-i", "input.cfg"], cwd=tmp_path, capture_output=True, text=True,
+                         timeout=600, env=dict(os.environ, OMP_NUM_THREADS="1"))
+    assert out.returncode == 0, out.stdout + out.stderr
+    ref = (GOLDEN / "dropin_cavitation_rc25.ref.txt").read_text()
+    for label in ("Thermalize", "Observe"):
+        got, want = labelled_rows(out.stdout, label), labelled_rows(ref, label)
+        assert got.shape == want.shape and got.shape[0] >= 2
+        assert np.allclose(got, want, rtol=2e-5, atol=2e-5), (label, np.abs(got - want).max())
+    dats = sorted(GOLDEN.glob("dropin_cavitation_rc25.conf*.dat"))
+    assert len(dats) == 5
+    for want_file in dats:
+        name = want_file.name.split(".", 1)[1]
+        got = np.frombuffer((tmp_path / name).read_bytes(), dtype=np.uint8).astype(int)
+        want = np.frombuffer(want_file.read_bytes(), dtype=np.uint8).astype(int)
+        assert got.shape == want.shape and got.sum() == want.sum()
+        assert np.abs(got - want).max() <= 1  # an atom within rounding of a grid face may land next door
