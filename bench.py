@@ -577,6 +577,8 @@ def main_ensemble(args, ws, rank, local):
     mdn = args.md_steps_per_step
     ens = M.Ensemble([(r.q, r.v, r.L) for r in reps], cutoff=2.5, time_step=0.005, precision=M.FP32_MIXED,
                      device=local)
+    if args.eager:
+        ens.set_graph_mode(False)
     for _ in range(args.warmup):
         ens.calculate(mdn)
     stream = torch.cuda.ExternalStream(ens.stream())

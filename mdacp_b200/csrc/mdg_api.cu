@@ -194,7 +194,7 @@ void launch_disp(mdg_handle *h, cudaStream_t s, double lag) {
   k_disp_max<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(h->a, h->box, n, lag);
   k_disp_collect<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(h->a, h->box, n,
                                                                    h->prm.check_list_length, lag);
-  k_disp_pairs<1024><<<1, 1024, 0, s>>>(h->a, h->box, lag);
+  k_disp_pairs<256><<<kPairParts, 256, 0, s>>>(h->a, h->box, lag);
 }
 
 // Ghost age at the skin check of a step: the previous step ended with a half

@@ -375,13 +375,71 @@ __global__ void __launch_bounds__(BLOCK) k_disp_collect(Arrays a, Box b, int n, 
   });
 }
 
-// Third pass, one block: expired if the copies found reach
-// min(total copies, CheckListLength), or if a pair of candidate copies that
-// was at least SearchLength apart at the last build is now inside the
-// cut-off (src/pairlist.cc:86-121).  Copies carry their shifts, so the
-// distances are the reference's direct differences.
+// Candidate copies staged in shared memory for the pair test: old and
+// current position of each, one array per axis so that consecutive lanes
+// read consecutive doubles.  960 copies (45 KB) covers the reference's
+// CheckListLength of 500 with room; longer lists are read from global memory.
+constexpr int kPairStage = 960;
+
+struct PairStage {
+  double o[3][kPairStage], n[3][kPairStage];
+};
+
+// The pair test of PairList::CheckByDisplacement (src/pairlist.cc:99-121)
+// over rows a = part, part + parts, ... of the candidate list: sets *found
+// if a pair of candidate copies (a < b) that was at least SearchLength apart
+// at the last build is now inside the cut-off.  Copies carry their shifts,
+// so the distances are the reference's direct differences.  The result is
+// an "any" over the pairs, so splitting the rows over blocks and the columns
+// over threads changes only the time.  l must be the same for every thread
+// of the block (the staging pass ends in a barrier).
+template <int BLOCK>
+__device__ __forceinline__ void candidate_pair_test(const CopyView &cv, const double L[3], const int2 *cand, int l,
+                                                    double lag, double sl2, double rc2, int part, int parts,
+                                                    PairStage &sm, volatile int *found) {
+  if (l <= kPairStage) {
+    for (int k = threadIdx.x; k < l; k += BLOCK) {
+      const int2 c = cand[k];
+      double o[3], p[3];
+      copy_positions(cv, L, c.x, c.y, lag, o, p);
+      for (int d = 0; d < 3; d++) {
+        sm.o[d][k] = o[d];
+        sm.n[d][k] = p[d];
+      }
+    }
+    __syncthreads();
+    for (int a = part; a < l - 1 && !*found; a += parts) {
+      const double o1[3] = {sm.o[0][a], sm.o[1][a], sm.o[2][a]};
+      const double n1[3] = {sm.n[0][a], sm.n[1][a], sm.n[2][a]};
+      for (int c = a + 1 + threadIdx.x; c < l; c += BLOCK) {
+        const double o2[3] = {sm.o[0][c], sm.o[1][c], sm.o[2][c]};
+        if (dist2(o1, o2) < sl2) continue;
+        const double n2[3] = {sm.n[0][c], sm.n[1][c], sm.n[2][c]};
+        if (dist2(n1, n2) < rc2) *found = 1;
+      }
+    }
+  } else {
+    for (int a = part; a < l - 1 && !*found; a += parts) {
+      double o1[3], n1[3];
+      copy_positions(cv, L, cand[a].x, cand[a].y, lag, o1, n1);
+      for (int c = a + 1 + threadIdx.x; c < l; c += BLOCK) {
+        double o2[3], n2[3];
+        copy_positions(cv, L, cand[c].x, cand[c].y, lag, o2, n2);
+        if (dist2(o1, o2) < sl2) continue;
+        if (dist2(n1, n2) < rc2) *found = 1;
+      }
+    }
+  }
+}
+
+// Third pass, kPairParts blocks sharing the rows: expired if the copies
+// found reach min(total copies, CheckListLength), or if the pair test finds
+// a pair (src/pairlist.cc:86-121).
+constexpr int kPairParts = 16;
+
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_disp_pairs(Arrays a, Box b, double lag) {
+  __shared__ PairStage sm;
   __shared__ volatile int found;
   if (threadIdx.x == 0) found = 0;
   __syncthreads();
@@ -392,18 +450,7 @@ __global__ void __launch_bounds__(BLOCK) k_disp_pairs(Arrays a, Box b, double la
     if (threadIdx.x == 0) found = 1;
   } else {
     const int l = min(st->cand_n, b.check_list_length);
-    for (int r = 0; r < l - 1 && !found; r++) {
-      const int2 e1 = a.cand[r];
-      double o1[3], n1[3];
-      copy_positions(copy_view(a), b.L, e1.x, e1.y, lag, o1, n1);
-      for (int c = r + 1 + threadIdx.x; c < l; c += BLOCK) {
-        const int2 e2 = a.cand[c];
-        double o2[3], n2[3];
-        copy_positions(copy_view(a), b.L, e2.x, e2.y, lag, o2, n2);
-        if (dist2(o1, o2) < b.sl2) continue;
-        if (dist2(n1, n2) < b.rc2) found = 1;
-      }
-    }
+    candidate_pair_test<BLOCK>(copy_view(a), b.L, a.cand, l, lag, b.sl2, b.rc2, blockIdx.x, gridDim.x, sm, &found);
   }
   __syncthreads();
   if (threadIdx.x == 0 && found) st->want_build = 1;

@@ -31,6 +31,7 @@ namespace {
 constexpr int kEB = 256;        // streaming kernels
 constexpr int kEF = 128;        // pair kernels
 constexpr int kEStepsPerGraph = 20;
+constexpr int kEPairParts = 8;  // blocks per replica in the candidate-pair test
 
 struct Rep {
   double L[3], hL[3], inv_cs[3], cs[3];
@@ -192,11 +193,13 @@ __global__ void __launch_bounds__(kEB) ke_disp_collect(Ens e) {
   });
 }
 
-// One block per replica: the candidate-pair test of PairList::CheckByDisplacement.
+// kEPairParts blocks per replica (blockIdx.y) share the rows of the
+// candidate-pair test of PairList::CheckByDisplacement.
 __global__ void __launch_bounds__(256) ke_disp_pairs(Ens e) {
   const int r = blockIdx.x;
   RepStatus &st = e.rs[r];
   if (!st.disp) return;
+  __shared__ PairStage sm;
   __shared__ volatile int found;
   if (threadIdx.x == 0) found = 0;
   __syncthreads();
@@ -207,18 +210,8 @@ __global__ void __launch_bounds__(256) ke_disp_pairs(Ens e) {
     if (threadIdx.x == 0) found = 1;
   } else {
     const int l = min(st.cand_n, e.cll);
-    const int2 *cand = e.cand + (size_t)r * e.cll;
-    const CopyView cv = ens_view(e);
-    for (int a = 0; a < l - 1 && !found; a++) {
-      double o1[3], n1[3];
-      copy_positions(cv, rep.L, cand[a].x, cand[a].y, e.lag, o1, n1);
-      for (int bb = a + 1 + threadIdx.x; bb < l; bb += blockDim.x) {
-        double o2[3], n2[3];
-        copy_positions(cv, rep.L, cand[bb].x, cand[bb].y, e.lag, o2, n2);
-        if (dist2(o1, o2) < e.sl2) continue;
-        if (dist2(n1, n2) < e.rc2) found = 1;
-      }
-    }
+    candidate_pair_test<256>(ens_view(e), rep.L, e.cand + (size_t)r * e.cll, l, e.lag, e.sl2, e.rc2, blockIdx.y,
+                             gridDim.y, sm, &found);
   }
   __syncthreads();
   if (threadIdx.x == 0 && found) st.want_build = 1;
@@ -709,7 +702,7 @@ void e_launch_disp(mdg_ensemble *x, cudaStream_t s) {
   Ens &e = x->e;
   ke_disp_max<<<nb(e.ntot, kEB), kEB, 0, s>>>(e);
   ke_disp_collect<<<nb(e.ntot, kEB), kEB, 0, s>>>(e);
-  ke_disp_pairs<<<e.nrep, 256, 0, s>>>(e);
+  ke_disp_pairs<<<dim3(e.nrep, kEPairParts), 256, 0, s>>>(e);
 }
 
 void e_launch_build(mdg_ensemble *x, cudaStream_t s) {
