@@ -201,6 +201,9 @@ def main():
     ap.add_argument("--no-force-error", action="store_true", help="skip the FP32-vs-FP64 force check")
     ap.add_argument("--drift-steps", type=int, default=2000,
                     help="NVE steps of the energy-drift comparison of the two paths (0: skip)")
+    ap.add_argument("--stage-atoms", type=int, default=0,
+                    help="FP32-mixed force: partner positions staged per 128-atom block in shared memory, "
+                         "at most this many atoms (0: gather from global memory, the default; -1: 2304)")
     ap.add_argument("--eager", action="store_true",
                     help="launch every kernel from the host instead of CUDA graphs (for profilers)")
     ap.add_argument("--config", choices=["c2", "c1", "c3", "c4", "c5"], default="c2",
@@ -220,6 +223,8 @@ def main():
     state, config = workload(args, rank)
     if args.impl == "reference":
         return main_reference(args, ws, rank, state, config)
+    if args.stage_atoms != 0:
+        config["force_stage_atoms"] = args.stage_atoms
     return main_mdg(args, ws, rank, local, state, config)
 
 
@@ -262,7 +267,8 @@ def metric_for(config):
 
 
 def system_kwargs(state, config, M):
-    kw = dict(cutoff=state.rc, time_step=state.dt, capacity=state.n)
+    kw = dict(cutoff=state.rc, time_step=state.dt, capacity=state.n,
+              stage_atoms=config.get("force_stage_atoms", 0))
     if config.get("thermostat") == "Langevin":
         kw.update(thermostat=M.LANGEVIN, aimed_temperature=config["temperature"],
                   heatbath_gamma=config["gamma"], seed=7)

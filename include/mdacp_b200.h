@@ -70,6 +70,9 @@ typedef struct {
   int max_neighbors;        /* neighbour-row capacity; 0 = derived from density */
   int device;               /* CUDA device ordinal */
   void *stream;             /* cudaStream_t to issue work on; NULL = handle-owned stream */
+  int stage_atoms;          /* FP32-mixed: partner positions staged in shared memory per
+                               128-atom block, at most this many atoms; 0 (default) = off,
+                               partners gathered from global memory; -1 = 2304 atoms */
 } mdg_params;
 
 /* Fills p with the reference defaults (SimulationInfo ctor, src/simulationinfo.cc:5-51). */

@@ -80,6 +80,7 @@ class Params(ctypes.Structure):
         ("max_neighbors", ctypes.c_int),
         ("device", ctypes.c_int),
         ("stream", ctypes.c_void_p),
+        ("stage_atoms", ctypes.c_int),
     ]
 
 
@@ -252,7 +253,7 @@ class System:
     def __init__(self, L, cutoff=2.5, time_step=0.005, capacity=None, precision=FP64,
                  thermostat=NVE, aimed_temperature=1.0, heatbath_tau=0.1, heatbath_gamma=0.1,
                  seed=0, buffer_length=0.3, check_list_length=500, max_neighbors=0, device=0,
-                 stream=None, n_hint=None):
+                 stream=None, n_hint=None, stage_atoms=0):
         self.lib = load_library()
         p = Params()
         self.lib.mdg_default_params(ctypes.byref(p))
@@ -271,6 +272,7 @@ class System:
         p.max_neighbors = int(max_neighbors)
         p.device = int(device)
         p.stream = stream
+        p.stage_atoms = int(stage_atoms)
         self.params = p
         h = _H()
         st = self.lib.mdg_create(ctypes.byref(p), ctypes.byref(h))

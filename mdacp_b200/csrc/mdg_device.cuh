@@ -16,6 +16,11 @@
 //                            walks 4 partners at a time; a self entry has r = 0
 //                            and is masked)
 //   qloc      float4[cap]    cell-local FP32 coordinates at the last build
+//   nbr16     uint2[maxnb/4][stride]  FP32-mixed only: the same rows as 16-bit
+//                            indices into the block's staged partner positions
+//                            (four per 8-byte load); see k_stage_plan
+//   stage_rng int4[blocks][kStageRanges]  per 128-atom block: the cell ranges
+//                            whose atoms the force pass stages in shared memory
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -27,6 +32,7 @@ constexpr int kErrTooFast = 2;
 constexpr int kErrInvalidPosition = 4;
 constexpr int kErrNonFinite = 8;
 constexpr int kErrTimeout = 16;
+constexpr int kErrStage = 32;  // a staged row index outside its block's stage (an inconsistent plan)
 
 // Geometry and force constants, passed by value to every kernel.
 struct Box {
@@ -104,6 +110,11 @@ struct Arrays {
   Status *st;
   int stride;         // column stride of nbr (>= cap, multiple of 32)
   int maxnb;          // neighbour-row capacity
+  // staged FP32 force (null / 0 when off)
+  int4 *stage_rng;    // per block: (first cell, end cell, first atom, offset in the block's stage)
+  int *stage_n;       // per block: ranges, -1 = partners gathered from global memory
+  uint2 *nbr16;       // rows as stage indices, four 16-bit entries per element
+  int stage_cap;      // atoms one block stages at most
 };
 
 // ------------------------------------------------------------------ helpers
@@ -456,6 +467,122 @@ __global__ void __launch_bounds__(BLOCK) k_disp_pairs(Arrays a, Box b, double la
   if (threadIdx.x == 0 && found) st->want_build = 1;
 }
 
+// ------------------------------------------------------ staged partners
+// The FP32-mixed force pass stages, per block of kStageBlock consecutive
+// atoms, the fixed-point positions of every atom in the union of the
+// block's 27-cell stencils in shared memory, and reads partners from there.
+// Atoms are in cell order, so that union is a few runs of consecutive cells
+// (the stencil rows of the block's home cells), i.e. a few runs of
+// consecutive atoms, which the pass copies with bulk asynchronous copies.
+// Rows hold, besides the global partner index, its index in the stage
+// (16 bits, four per 8-byte element).  The pair terms and their order are
+// the global-gather pass's; only where the positions are read from changes.
+constexpr int kStageBlock = 128;
+constexpr int kStageRanges = 32;
+constexpr int kStageRaw = 96;  // stencil-row cell runs per block before merging
+
+// Offset from a global atom index to its stage index, for an atom of cell nc:
+// the plan range that holds nc (ranges are sorted by first cell).
+__device__ __forceinline__ int stage_shift(const int4 *plan, int npl, int nc) {
+  int lo = 0, hi = npl - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (plan[mid].x <= nc) lo = mid;
+    else hi = mid - 1;
+  }
+  return plan[lo].w - plan[lo].z;
+}
+
+// Entry k of atom i's staged row: four 16-bit entries per uint2, written
+// when the fourth arrives (rows are padded to a multiple of 4).
+__device__ __forceinline__ void stage_entry(uint2 *nbr16, int stride, int i, int k, int v, unsigned &g0,
+                                            unsigned &g1) {
+  const unsigned val = (unsigned)v & 0xffffu;
+  switch (k & 3) {
+    case 0: g0 = val; g1 = 0u; break;
+    case 1: g0 |= val << 16; break;
+    case 2: g1 = val; break;
+    default:
+      g1 |= val << 16;
+      nbr16[(size_t)(k >> 2) * stride + i] = make_uint2(g0, g1);
+  }
+}
+
+// Rebuild, after the permutation and the cell scan: the stage plan of every
+// block of kStageBlock atoms, one thread per block.  The block's home cells
+// lie in [cell of its first atom, cell of its last atom]; each run of them
+// along x contributes, per (dz, dy), the cells x-1 .. x+1 of that row (one
+// or two runs with the periodic wrap).  The runs are sorted and merged; a
+// block that needs more than kStageRanges runs or more than stage_cap atoms
+// is marked -1 and gathers its partners from global memory.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_stage_plan(Arrays a, Box b, int n) {
+  const int blk = blockIdx.x * BLOCK + threadIdx.x;
+  const int nblk = (n + kStageBlock - 1) / kStageBlock;
+  if (blk >= nblk || a.st->error) return;
+  const int i0 = blk * kStageBlock, i1 = min(n, i0 + kStageBlock) - 1;
+  const int c_first = a.cell_tmp[i0], c_last = a.cell_tmp[i1];
+  const int ms0 = b.ms[0], ms1 = b.ms[1], ms2 = b.ms[2];
+  int2 run[kStageRaw];
+  int nrun = 0;
+  bool over = false;
+  for (int c = c_first; c <= c_last && !over;) {
+    const int xa = c % ms0, y = (c / ms0) % ms1, z = c / (ms0 * ms1);
+    const int xb = min(ms0 - 1, xa + (c_last - c));
+    c += xb - xa + 1;
+    if (nrun + 18 > kStageRaw) {
+      over = true;
+      break;
+    }
+    const int lo = xa - 1, hi = xb + 1;  // inclusive, before the wrap
+    int s0, e0, s1 = 0, e1 = 0;
+    if (hi - lo + 1 >= ms0) {
+      s0 = 0; e0 = ms0;
+    } else if (lo < 0) {
+      s0 = 0; e0 = hi + 1; s1 = lo + ms0; e1 = ms0;
+    } else if (hi >= ms0) {
+      s0 = 0; e0 = hi - ms0 + 1; s1 = lo; e1 = ms0;
+    } else {
+      s0 = lo; e0 = hi + 1;
+    }
+    for (int dz = -1; dz <= 1; dz++) {
+      const int zz = (z + dz + ms2) % ms2;
+      for (int dy = -1; dy <= 1; dy++) {
+        const int base = (zz * ms1 + (y + dy + ms1) % ms1) * ms0;
+        run[nrun++] = make_int2(base + s0, base + e0);
+        if (e1 > s1) run[nrun++] = make_int2(base + s1, base + e1);
+      }
+    }
+  }
+  int m = 0;
+  if (!over) {
+    for (int k = 1; k < nrun; k++) {  // insertion sort by first cell
+      const int2 x = run[k];
+      int j = k - 1;
+      while (j >= 0 && run[j].x > x.x) {
+        run[j + 1] = run[j];
+        j--;
+      }
+      run[j + 1] = x;
+    }
+    for (int k = 0; k < nrun; k++) {  // merge overlapping and touching runs
+      if (m > 0 && run[k].x <= run[m - 1].y) run[m - 1].y = max(run[m - 1].y, run[k].y);
+      else run[m++] = run[k];
+    }
+    over = m > kStageRanges;
+  }
+  int total = 0;
+  if (!over) {
+    for (int r = 0; r < m; r++) {
+      const int first = a.cell_start[run[r].x];
+      a.stage_rng[blk * kStageRanges + r] = make_int4(run[r].x, run[r].y, first, total);
+      total += a.cell_start[run[r].y] - first;
+    }
+    over = total > a.stage_cap;
+  }
+  a.stage_n[blk] = over ? -1 : m;
+}
+
 // Rebuild 1/6: wrap into [0,L] (Variables::AdjustPeriodicBoundary,
 // src/variables.cc:63-84), validity check, cell index and rank inside the cell.
 template <int BLOCK>
@@ -678,6 +805,27 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
   const int i = blockIdx.x * BLOCK + threadIdx.x;
   int cnt = 0;
+  // staged rows (FP32-mixed): the block's stage plan, see k_stage_plan
+  __shared__ int4 plan[kStageRanges];
+  __shared__ int nplan;
+  __shared__ int nstaged;
+  if (threadIdx.x == 0) {
+    int m = (a.nbr16 && BLOCK == kStageBlock) ? a.stage_n[blockIdx.x] : -1;
+    nplan = (m > 0 && m <= kStageRanges) ? m : -1;
+  }
+  __syncthreads();
+  const int npl = nplan;
+  if ((int)threadIdx.x < npl) plan[threadIdx.x] = a.stage_rng[blockIdx.x * kStageRanges + threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x == 0 && npl > 0) {
+    const int4 last = plan[npl - 1];
+    nstaged = last.w + a.cell_start[last.y] - last.z;
+  }
+  __syncthreads();
+  // a stage index outside the stage would be a plan that misses a stencil
+  // cell: flagged, and the entry points at the atom's own slot 0 instead
+  const int staged_atoms = npl > 0 ? nstaged : 0;
+  unsigned g0 = 0u, g1 = 0u;  // the row's current group of four stage indices
   if (i < n && !a.st->error) {
     const float4 li = a.qloc[i];
     const int c = a.cell_tmp[i];
@@ -702,6 +850,7 @@ __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
           const int nc = (z * b.ms[1] + y) * b.ms[0] + x;
           const int beg = a.cell_start[nc], end = a.cell_start[nc + 1];
           const int need = needed_strips(sx, sy, sz);
+          const int shift = npl > 0 ? stage_shift(plan, npl, nc) : 0;
           for (int j = beg; j < end; j++) {
             const float4 lj = a.qloc[j];
             const float ex = lj.x + bx, ey = lj.y + by, ez = lj.z + bz;
@@ -709,7 +858,17 @@ __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
             if (r2 > hi || j == i) continue;
             if (need && (a.mult[j] & need) != need) continue;
             if (r2 >= lo && !within_search_exact(a.q[i], a.q[j], sx, sy, sz, b.sl2)) continue;
-            if (cnt < maxnb) a.nbr[(size_t)cnt * stride + i] = j;
+            if (cnt < maxnb) {
+              a.nbr[(size_t)cnt * stride + i] = j;
+              if (npl > 0) {
+                int v = j + shift;
+                if (v < 0 || v >= staged_atoms) {
+                  atomicOr(&a.st->error, kErrStage);
+                  v = 0;
+                }
+                stage_entry(a.nbr16, stride, i, cnt, v, g0, g1);
+              }
+            }
             cnt++;
           }
         }
@@ -719,7 +878,15 @@ __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
     if (cnt > maxnb) {
       atomicOr(&a.st->error, kErrCapacity);
     } else {
-      for (int k = cnt; k < ((cnt + 3) & ~3); k++) a.nbr[(size_t)k * stride + i] = i;
+      int self = npl > 0 ? i + stage_shift(plan, npl, c) : 0;
+      if (npl > 0 && (self < 0 || self >= staged_atoms)) {
+        atomicOr(&a.st->error, kErrStage);
+        self = 0;
+      }
+      for (int k = cnt; k < ((cnt + 3) & ~3); k++) {
+        a.nbr[(size_t)k * stride + i] = i;
+        if (npl > 0) stage_entry(a.nbr16, stride, i, k, self, g0, g1);
+      }
     }
   }
   const int wmax = __reduce_max_sync(0xffffffffu, cnt);
@@ -1038,21 +1205,158 @@ __device__ __forceinline__ void lj_pair_fp32(const int4 &pi, const int4 &pj, flo
   fz = fmaf(df, dz, fz);
 }
 
+// The per-atom end of an FP32-mixed force pass: the FP64 kick and, with
+// DRIFT, the second half drift (DRIFT == 2 also this step's first half
+// drift of the atom itself and the pack of the next step's first-drift
+// position into qf_next).
+template <int MODE, int DRIFT>
+__device__ __forceinline__ void fp32_finish(Arrays &a, const Box &b, const Thermo &th, int i, double Fx, double Fy,
+                                            double Fz, int4 *qf_next, double &v2, double &ke) {
+  const double dt = (MODE == kForceOut) ? 1.0 : b.dt;
+  const double dt2 = b.dt * 0.5;
+  double4 q = a.q[i];
+  if (DRIFT == 2) {
+    // this step's first half drift (the neighbours' copies in qf already have it)
+    const double4 v0 = a.v[i];
+    q.x = dadd(q.x, dmul(v0.x, dt2));
+    q.y = dadd(q.y, dmul(v0.y, dt2));
+    q.z = dadd(q.z, dmul(v0.z, dt2));
+  }
+  finish_atom<MODE>(a, b, th, i, Fx * dt, Fy * dt, Fz * dt, v2, ke);
+  if (DRIFT) {
+    const double4 v = a.v[i];
+    q.x = dadd(q.x, dmul(v.x, dt2));
+    q.y = dadd(q.y, dmul(v.y, dt2));
+    q.z = dadd(q.z, dmul(v.z, dt2));
+    a.q[i] = q;
+    v2 = dadd(dadd(dmul(v.x, v.x), dmul(v.y, v.y)), dmul(v.z, v.z));
+    if (!isfinite(v2) || !isfinite(q.x + q.y + q.z)) atomicOr(&a.st->error, kErrNonFinite);
+    if (DRIFT == 2) {
+      // the next step's first half drift, packed for its force pass
+      qf_next[i] = make_int4(fixed_coord(dadd(q.x, dmul(v.x, dt2)), b.L[0]),
+                             fixed_coord(dadd(q.y, dmul(v.y, dt2)), b.L[1]),
+                             fixed_coord(dadd(q.z, dmul(v.z, dt2)), b.L[2]), 0);
+    }
+  }
+}
+
+// Row sum of atom i from the global fixed-point copy: rows are padded to a
+// multiple of 4, so the row is walked four partners at a time without
+// per-lane masks, with the indices of the next eight partners already in
+// flight (the list is the one stream from HBM, so its loads are issued two
+// groups ahead); FP32 partial sums over 8 partners are folded into the FP64
+// sums.
+__device__ __forceinline__ void fp32_row_global(const Arrays &a, const Box &b, const int4 *qf, int i,
+                                                const int4 &pi, int nn4, double &Fx, double &Fy, double &Fz) {
+  const float sx = b.fix_scale[0], sy = b.fix_scale[1], sz = b.fix_scale[2];
+  const unsigned rc2_bits = __float_as_uint(b.rc2f);
+  const float c2x8 = b.c2x8f;
+  const int *row = a.nbr + i;
+  const int st = a.stride;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  int n0 = i, n1 = i, n2 = i, n3 = i;
+  int m0 = i, m1 = i, m2 = i, m3 = i;
+  if (nn4 > 0) {
+    n0 = __ldg(row);
+    n1 = __ldg(row + st);
+    n2 = __ldg(row + 2 * st);
+    n3 = __ldg(row + 3 * st);
+  }
+  if (nn4 > 4) {
+    m0 = __ldg(row + 4 * st);
+    m1 = __ldg(row + 5 * st);
+    m2 = __ldg(row + 6 * st);
+    m3 = __ldg(row + 7 * st);
+  }
+  for (int k = 0; k < nn4; k += 4) {
+    const int4 p0 = __ldg(qf + n0);
+    const int4 p1 = __ldg(qf + n1);
+    const int4 p2 = __ldg(qf + n2);
+    const int4 p3 = __ldg(qf + n3);
+    n0 = m0;
+    n1 = m1;
+    n2 = m2;
+    n3 = m3;
+    if (k + 8 < nn4) {
+      const int *r = row + (size_t)(k + 8) * st;
+      m0 = __ldg(r);
+      m1 = __ldg(r + st);
+      m2 = __ldg(r + 2 * st);
+      m3 = __ldg(r + 3 * st);
+    }
+    lj_pair_fp32(pi, p0, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
+    lj_pair_fp32(pi, p1, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
+    lj_pair_fp32(pi, p2, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
+    lj_pair_fp32(pi, p3, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
+    if (k & 4) {
+      Fx += (double)fx;
+      Fy += (double)fy;
+      Fz += (double)fz;
+      fx = fy = fz = 0.f;
+    }
+  }
+  Fx += (double)fx;
+  Fy += (double)fy;
+  Fz += (double)fz;
+}
+
+// The same row sum from the block's stage in shared memory: one 8-byte load
+// brings four stage indices; the next two groups are in flight.
+__device__ __forceinline__ unsigned stage_index(unsigned v, unsigned nstage, bool &bad) {
+  const bool out = v >= nstage;
+  bad |= out;
+  return out ? 0u : v;
+}
+
+__device__ __forceinline__ void fp32_row_staged(const Arrays &a, const Box &b, const int4 *pos, unsigned nstage,
+                                                int i, const int4 &pi, int nn4, double &Fx, double &Fy,
+                                                double &Fz) {
+  const float sx = b.fix_scale[0], sy = b.fix_scale[1], sz = b.fix_scale[2];
+  const unsigned rc2_bits = __float_as_uint(b.rc2f);
+  const float c2x8 = b.c2x8f;
+  const uint2 *row = a.nbr16 + i;
+  const int st = a.stride;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  uint2 g = make_uint2(0u, 0u), gn = make_uint2(0u, 0u);
+  bool bad = false;  // an index outside the stage: flagged, the read skipped
+  if (nn4 > 0) g = __ldg(row);
+  if (nn4 > 4) gn = __ldg(row + st);
+  for (int k = 0; k < nn4; k += 4) {
+    const int4 p0 = pos[stage_index(g.x & 0xffffu, nstage, bad)];
+    const int4 p1 = pos[stage_index(g.x >> 16, nstage, bad)];
+    const int4 p2 = pos[stage_index(g.y & 0xffffu, nstage, bad)];
+    const int4 p3 = pos[stage_index(g.y >> 16, nstage, bad)];
+    g = gn;
+    if (k + 8 < nn4) gn = __ldg(row + (size_t)((k + 8) >> 2) * st);
+    lj_pair_fp32(pi, p0, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
+    lj_pair_fp32(pi, p1, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
+    lj_pair_fp32(pi, p2, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
+    lj_pair_fp32(pi, p3, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
+    if (k & 4) {
+      Fx += (double)fx;
+      Fy += (double)fy;
+      Fz += (double)fz;
+      fx = fy = fz = 0.f;
+    }
+  }
+  Fx += (double)fx;
+  Fy += (double)fy;
+  Fz += (double)fz;
+  if (bad) atomicOr(&a.st->error, kErrStage);
+}
+
 // FP32-mixed force kick.  Displacements come from the fixed-point copy (no
-// ghost atoms, no shift codes).  Rows are padded to a multiple of 4, so the
-// row is walked four partners at a time without per-lane masks, with the
-// indices of the next eight partners already in flight (the list is the one
-// stream from HBM, so its loads are issued two groups ahead); FP32 partial sums over 8 partners are
-// folded into an FP64 per-atom sum; the kick is FP64.  With DRIFT the second
-// half drift q += v dt/2 and the |v| maximum of the step are done in the
-// same pass: this kernel reads only the fixed-point copy, so moving q here
-// races with no other thread.  DRIFT == 2 is the whole NVE step in one pass:
-// qf holds every atom's position after this step's first half drift (packed
-// by the previous step's pass, or by k_pack_half after a rebuild); the
-// kernel applies that drift to its own atom, kicks, drifts again and packs
-// the next step's first-drift position into qf_next (the other buffer, so
-// no thread overwrites a copy that another still reads).  The arithmetic is
-// the separate drift kernels', operation for operation.
+// ghost atoms, no shift codes); the row sum is fp32_row_global's and the
+// kick is FP64.  With DRIFT the second half drift q += v dt/2 and the |v|
+// maximum of the step are done in the same pass: this kernel reads only the
+// fixed-point copy, so moving q here races with no other thread.  DRIFT == 2
+// is the whole NVE step in one pass: qf holds every atom's position after
+// this step's first half drift (packed by the previous step's pass, or by
+// k_pack_half after a rebuild); the kernel applies that drift to its own
+// atom, kicks, drifts again and packs the next step's first-drift position
+// into qf_next (the other buffer, so no thread overwrites a copy that
+// another still reads).  The arithmetic is the separate drift kernels',
+// operation for operation.
 template <int BLOCK, int MODE, int DRIFT>
 __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Thermo th, const int4 *qf,
                                                       int4 *qf_next) {
@@ -1066,83 +1370,134 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Th
   if (i < n && !a.st->error) {
     const int4 pi = qf[i];
     const int nn4 = (a.nnbr[i] + 3) & ~3;
-    const float sx = b.fix_scale[0], sy = b.fix_scale[1], sz = b.fix_scale[2];
-    const unsigned rc2_bits = __float_as_uint(b.rc2f);
-    const float c2x8 = b.c2x8f;
-    const int *row = a.nbr + i;
-    const int st = a.stride;
     double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-    float fx = 0.f, fy = 0.f, fz = 0.f;
-    int n0 = i, n1 = i, n2 = i, n3 = i;
-    int m0 = i, m1 = i, m2 = i, m3 = i;
-    if (nn4 > 0) {
-      n0 = __ldg(row);
-      n1 = __ldg(row + st);
-      n2 = __ldg(row + 2 * st);
-      n3 = __ldg(row + 3 * st);
-    }
-    if (nn4 > 4) {
-      m0 = __ldg(row + 4 * st);
-      m1 = __ldg(row + 5 * st);
-      m2 = __ldg(row + 6 * st);
-      m3 = __ldg(row + 7 * st);
-    }
-    for (int k = 0; k < nn4; k += 4) {
-      const int4 p0 = __ldg(qf + n0);
-      const int4 p1 = __ldg(qf + n1);
-      const int4 p2 = __ldg(qf + n2);
-      const int4 p3 = __ldg(qf + n3);
-      n0 = m0;
-      n1 = m1;
-      n2 = m2;
-      n3 = m3;
-      if (k + 8 < nn4) {
-        const int *r = row + (size_t)(k + 8) * st;
-        m0 = __ldg(r);
-        m1 = __ldg(r + st);
-        m2 = __ldg(r + 2 * st);
-        m3 = __ldg(r + 3 * st);
+    fp32_row_global(a, b, qf, i, pi, nn4, Fx, Fy, Fz);
+    fp32_finish<MODE, DRIFT>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
+  }
+  if (MODE == kKickLangevin || DRIFT) warp_max_to(&a.st->vmax2_bits, v2);
+  if (MODE == kKickNoseHoover) {
+    double s[1] = {ke};
+    block_sum_to<BLOCK, 1>(s, a.partials);
+  }
+}
+
+// ---------------------------------------------- mbarrier and bulk copies
+// (PTX ISA: mbarrier, cp.async.bulk; sm_90 and later)
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned)
+// from global to shared memory, completing on the mbarrier's transaction
+// count.  A plain load: no multicast.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Waits for the mbarrier's phase `parity` to complete, for at most
+// `limit` clock cycles; false if it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > limit) return false;
+  }
+}
+
+// About one second at the B200's clocks: a stage copy takes microseconds.
+constexpr long long kStageWaitCycles = 2000000000ll;
+
+// The staged FP32-mixed pass: k_force_fp32 with the partners' positions read
+// from the block's stage (k_stage_plan) in dynamic shared memory, which one
+// thread fills with one bulk copy per plan range while the others wait on an
+// mbarrier.  Blocks without a plan (-1) gather from global memory.  If the
+// wait gives up (kStageWaitCycles), the block sets kErrTimeout, waits once
+// more for its copies in flight, and kicks no atom.
+template <int BLOCK, int MODE, int DRIFT>
+__global__ void __launch_bounds__(BLOCK) k_force_fp32_staged(Arrays a, Box b, int n, Thermo th, const int4 *qf,
+                                                             int4 *qf_next) {
+  extern __shared__ __align__(16) int4 pos[];
+  __shared__ __align__(8) uint64_t bar;
+  static_assert(BLOCK == kStageBlock, "stage plans are per kStageBlock atoms");
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  double v2 = 0.0, ke = 0.0;
+  if (DRIFT == 2 && MODE == kKick && i == 0 && !a.st->error) {
+    a.st->steps++;
+    a.st->sim_time += b.dt;
+  }
+  // thread 0 checks the plan against the stage and the atom count (a plan
+  // left from an earlier layout is never copied) and fills the stage
+  __shared__ int staged;
+  __shared__ unsigned nstage;
+  uint32_t total = 0;
+  if (threadIdx.x == 0) {
+    const int npl = a.stage_n[blockIdx.x];
+    int use = npl > 0 && npl <= kStageRanges && !a.st->error;
+    const int4 *plan = a.stage_rng + (size_t)blockIdx.x * kStageRanges;
+    for (int r = 0; use && r < npl; r++) {
+      const int4 pr = plan[r];
+      if (pr.x < 0 || pr.y > b.ncell || pr.x >= pr.y) {
+        use = 0;
+        break;
       }
-      lj_pair_fp32(pi, p0, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-      lj_pair_fp32(pi, p1, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-      lj_pair_fp32(pi, p2, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-      lj_pair_fp32(pi, p3, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-      if (k & 4) {
-        Fx += (double)fx;
-        Fy += (double)fy;
-        Fz += (double)fz;
-        fx = fy = fz = 0.f;
+      const int cnt = a.cell_start[pr.y] - pr.z;
+      if (cnt < 0 || pr.z < 0 || pr.z + cnt > n || pr.w != (int)total || pr.w + cnt > a.stage_cap) use = 0;
+      // bulk copies start on 16-byte boundaries at both ends
+      if (cnt > 0 && (((smem_addr(pos + pr.w) | (uint32_t)(uintptr_t)(qf + pr.z)) & 15u) != 0u)) use = 0;
+      total += (uint32_t)cnt;
+    }
+    if (!use && npl > 0 && npl <= kStageRanges && !a.st->error) atomicOr(&a.st->error, kErrStage);
+    if (use) mbar_init(&bar, 1);
+    staged = use;
+    nstage = use ? total : 0u;
+  }
+  __syncthreads();
+  const bool use_stage = staged != 0;
+  bool ok = true;
+  if (use_stage) {
+    if (threadIdx.x == 0) {
+      const int npl = a.stage_n[blockIdx.x];
+      const int4 *plan = a.stage_rng + (size_t)blockIdx.x * kStageRanges;
+      mbar_arrive_expect_tx(&bar, total * (uint32_t)sizeof(int4));
+      for (int r = 0; r < npl; r++) {
+        const int4 pr = plan[r];
+        const int cnt = a.cell_start[pr.y] - pr.z;
+        if (cnt > 0) bulk_load(pos + pr.w, qf + pr.z, (uint32_t)cnt * (uint32_t)sizeof(int4), &bar);
       }
     }
-    Fx += (double)fx;
-    Fy += (double)fy;
-    Fz += (double)fz;
-    const double dt = (MODE == kForceOut) ? 1.0 : b.dt;
-    const double dt2 = b.dt * 0.5;
-    double4 q = a.q[i];
-    if (DRIFT == 2) {
-      // this step's first half drift (the neighbours' copies in qf already have it)
-      const double4 v0 = a.v[i];
-      q.x = dadd(q.x, dmul(v0.x, dt2));
-      q.y = dadd(q.y, dmul(v0.y, dt2));
-      q.z = dadd(q.z, dmul(v0.z, dt2));
+    ok = mbar_wait(&bar, 0, kStageWaitCycles);
+    if (!ok) {
+      atomicOr(&a.st->error, kErrTimeout);
+      mbar_wait(&bar, 0, kStageWaitCycles);
     }
-    finish_atom<MODE>(a, b, th, i, Fx * dt, Fy * dt, Fz * dt, v2, ke);
-    if (DRIFT) {
-      const double4 v = a.v[i];
-      q.x = dadd(q.x, dmul(v.x, dt2));
-      q.y = dadd(q.y, dmul(v.y, dt2));
-      q.z = dadd(q.z, dmul(v.z, dt2));
-      a.q[i] = q;
-      v2 = dadd(dadd(dmul(v.x, v.x), dmul(v.y, v.y)), dmul(v.z, v.z));
-      if (!isfinite(v2) || !isfinite(q.x + q.y + q.z)) atomicOr(&a.st->error, kErrNonFinite);
-      if (DRIFT == 2) {
-        // the next step's first half drift, packed for its force pass
-        qf_next[i] = make_int4(fixed_coord(dadd(q.x, dmul(v.x, dt2)), b.L[0]),
-                               fixed_coord(dadd(q.y, dmul(v.y, dt2)), b.L[1]),
-                               fixed_coord(dadd(q.z, dmul(v.z, dt2)), b.L[2]), 0);
-      }
-    }
+  }
+  if (ok && i < n && !a.st->error) {
+    const int4 pi = qf[i];
+    const int nn4 = (a.nnbr[i] + 3) & ~3;
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    if (use_stage) fp32_row_staged(a, b, pos, nstage, i, pi, nn4, Fx, Fy, Fz);
+    else fp32_row_global(a, b, qf, i, pi, nn4, Fx, Fy, Fz);
+    fp32_finish<MODE, DRIFT>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
   }
   if (MODE == kKickLangevin || DRIFT) warp_max_to(&a.st->vmax2_bits, v2);
   if (MODE == kKickNoseHoover) {
