@@ -332,9 +332,11 @@ def timed_run(sys_, args, dist, device, torch):
     info1 = sys_.info()
     fms, flaunch, klaunch = sys_.kernel_time()
     sys_.set_kernel_timing(False)
-    # kernels inside the conditional branches: a rebuild is 10 kernels, a
-    # displacement check 4 (three passes and the rebuild decision)
-    launches = klaunch + 10 * (info1["rebuilds"] - info0["rebuilds"]) + 4 * (
+    # kernels inside the conditional branches: a rebuild is 10 kernels (11
+    # with the staged FP32 force pass's plan), a displacement check 4 (three
+    # passes and the rebuild decision)
+    staged = sys_.params.precision != 0 and sys_.params.stage_atoms != 0
+    launches = klaunch + (11 if staged else 10) * (info1["rebuilds"] - info0["rebuilds"]) + 4 * (
         info1["displacement_checks"] - info0["displacement_checks"])
     return ms, fms, flaunch, launches, info0, info1
 

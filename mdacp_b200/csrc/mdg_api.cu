@@ -218,6 +218,9 @@ double step_lag(const mdg_handle *h) {
 // Pairlist rebuild (MDManager::MakePairList).
 // pack: where to put the coming step's first-drift positions after the
 // rebuild (the fused FP32 NVE step), or nullptr.
+// Kernels of one rebuild (launch_build).
+int build_kernels(const mdg_handle *h) { return h->a.stage_cap > 0 ? 11 : 10; }
+
 void launch_build(mdg_handle *h, cudaStream_t s, int4 *pack = nullptr) {
   const int n = h->n;
   Arrays &a = h->a;
@@ -238,8 +241,10 @@ void launch_build(mdg_handle *h, cudaStream_t s, int4 *pack = nullptr) {
   if (a.stage_cap > 0) {
     static_assert(kForceBlock == kStageBlock, "the build writes stage rows per force block");
     k_stage_plan<kBlock><<<blocks_for(blocks_for(n, kStageBlock), kBlock), kBlock, 0, s>>>(a, h->box, n);
+    k_build<kForceBlock, true><<<blocks_for(n, kForceBlock), kForceBlock, 0, s>>>(a, h->box, n);
+  } else {
+    k_build<kForceBlock, false><<<blocks_for(n, kForceBlock), kForceBlock, 0, s>>>(a, h->box, n);
   }
-  k_build<kForceBlock><<<blocks_for(n, kForceBlock), kForceBlock, 0, s>>>(a, h->box, n);
   k_build_done<<<1, 32, 0, s>>>(a, h->box);
 }
 
@@ -497,7 +502,7 @@ mdg_status step_eager(mdg_handle *h) {
   const int parity = h->fix_buf > 0 ? 1 : 0;
   if (flags[1]) {
     launch_build(h, h->stream, fused_step(h) ? fix_buffer(h, parity) : nullptr);
-    h->kernel_launches += 11;
+    h->kernel_launches += build_kernels(h);
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (h->timing) {
@@ -535,7 +540,7 @@ mdg_status ensure_list(mdg_handle *h) {
   h->fix_buf = -1;  // the rebuild renumbers the atoms
   for (int attempt = 0; attempt < 4; attempt++) {
     launch_build(h, h->stream);
-    h->kernel_launches += 11;
+    h->kernel_launches += build_kernels(h);
     CUDA_TRY(h, cudaGetLastError());
     r = read_status(h, &st);
     if (r) return r;

@@ -801,30 +801,35 @@ __device__ __forceinline__ bool within_search_exact(const double4 &qi, const dou
 // exact FP64 test, so the pair set is the reference's bit for bit.  Row
 // order: cells in (dz,dy,dx) order, slots ascending; rows padded with the
 // atom's own index to a multiple of 4.
-template <int BLOCK>
+template <int BLOCK, bool STAGE>
 __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
   const int i = blockIdx.x * BLOCK + threadIdx.x;
   int cnt = 0;
-  // staged rows (FP32-mixed): the block's stage plan, see k_stage_plan
-  __shared__ int4 plan[kStageRanges];
+  // STAGE: also the rows as stage indices (FP32-mixed staged force), from
+  // the block's stage plan, see k_stage_plan
+  __shared__ int4 plan[STAGE ? kStageRanges : 1];
   __shared__ int nplan;
   __shared__ int nstaged;
-  if (threadIdx.x == 0) {
-    int m = (a.nbr16 && BLOCK == kStageBlock) ? a.stage_n[blockIdx.x] : -1;
-    nplan = (m > 0 && m <= kStageRanges) ? m : -1;
+  int npl = -1, staged_atoms = 0;
+  if (STAGE) {
+    static_assert(!STAGE || BLOCK == kStageBlock, "stage plans are per kStageBlock atoms");
+    if (threadIdx.x == 0) {
+      const int m = a.nbr16 ? a.stage_n[blockIdx.x] : -1;
+      nplan = (m > 0 && m <= kStageRanges) ? m : -1;
+    }
+    __syncthreads();
+    npl = nplan;
+    if ((int)threadIdx.x < npl) plan[threadIdx.x] = a.stage_rng[blockIdx.x * kStageRanges + threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x == 0 && npl > 0) {
+      const int4 last = plan[npl - 1];
+      nstaged = last.w + a.cell_start[last.y] - last.z;
+    }
+    __syncthreads();
+    // a stage index outside the stage would be a plan that misses a stencil
+    // cell: flagged, and the entry points at the atom's own slot 0 instead
+    staged_atoms = npl > 0 ? nstaged : 0;
   }
-  __syncthreads();
-  const int npl = nplan;
-  if ((int)threadIdx.x < npl) plan[threadIdx.x] = a.stage_rng[blockIdx.x * kStageRanges + threadIdx.x];
-  __syncthreads();
-  if (threadIdx.x == 0 && npl > 0) {
-    const int4 last = plan[npl - 1];
-    nstaged = last.w + a.cell_start[last.y] - last.z;
-  }
-  __syncthreads();
-  // a stage index outside the stage would be a plan that misses a stencil
-  // cell: flagged, and the entry points at the atom's own slot 0 instead
-  const int staged_atoms = npl > 0 ? nstaged : 0;
   unsigned g0 = 0u, g1 = 0u;  // the row's current group of four stage indices
   if (i < n && !a.st->error) {
     const float4 li = a.qloc[i];
@@ -850,7 +855,7 @@ __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
           const int nc = (z * b.ms[1] + y) * b.ms[0] + x;
           const int beg = a.cell_start[nc], end = a.cell_start[nc + 1];
           const int need = needed_strips(sx, sy, sz);
-          const int shift = npl > 0 ? stage_shift(plan, npl, nc) : 0;
+          const int shift = (STAGE && npl > 0) ? stage_shift(plan, npl, nc) : 0;
           for (int j = beg; j < end; j++) {
             const float4 lj = a.qloc[j];
             const float ex = lj.x + bx, ey = lj.y + by, ez = lj.z + bz;
@@ -860,7 +865,7 @@ __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
             if (r2 >= lo && !within_search_exact(a.q[i], a.q[j], sx, sy, sz, b.sl2)) continue;
             if (cnt < maxnb) {
               a.nbr[(size_t)cnt * stride + i] = j;
-              if (npl > 0) {
+              if (STAGE && npl > 0) {
                 int v = j + shift;
                 if (v < 0 || v >= staged_atoms) {
                   atomicOr(&a.st->error, kErrStage);
@@ -878,14 +883,14 @@ __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
     if (cnt > maxnb) {
       atomicOr(&a.st->error, kErrCapacity);
     } else {
-      int self = npl > 0 ? i + stage_shift(plan, npl, c) : 0;
-      if (npl > 0 && (self < 0 || self >= staged_atoms)) {
+      int self = (STAGE && npl > 0) ? i + stage_shift(plan, npl, c) : 0;
+      if (STAGE && npl > 0 && (self < 0 || self >= staged_atoms)) {
         atomicOr(&a.st->error, kErrStage);
         self = 0;
       }
       for (int k = cnt; k < ((cnt + 3) & ~3); k++) {
         a.nbr[(size_t)k * stride + i] = i;
-        if (npl > 0) stage_entry(a.nbr16, stride, i, k, self, g0, g1);
+        if (STAGE && npl > 0) stage_entry(a.nbr16, stride, i, k, self, g0, g1);
       }
     }
   }
