@@ -589,20 +589,34 @@ def main_ensemble(args, ws, rank, local):
         ens.set_graph_mode(False)
     for _ in range(args.warmup):
         ens.calculate(mdn)
+    ens.set_kernel_timing(True)
     stream = torch.cuda.ExternalStream(ens.stream())
+    sampler = ClockSampler(local)
     barrier(dist, device)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    sampler.start()
     e0.record(stream)
     for _ in range(args.steps):
         ens.calculate(mdn)
     e1.record(stream)
     e1.synchronize()
+    clocks = sampler.stop()
     ms = max_over_ranks(dist, e0.elapsed_time(e1), device)
     value = ws * ntot * args.steps * mdn / (ms * 1e-3)
+    fms, flaunch, launches = ens.kernel_time()
+    ens.set_kernel_timing(False)
+    entries, pairs = ens.list_stats()
     rb, _ = ens.rebuilds()
     ens.close()
+    # roofline of the ensemble's FP32 force pass (kick + second half drift,
+    # all replicas in one launch): own fixed-point copy, row length, list,
+    # velocity and position read and write
+    force_bytes = ntot * (16 + 4 + 64 + 64) + 4 * entries
+    avg_ms = fms / max(1, flaunch)
+    achieved = force_bytes / (avg_ms * 1e-3) / 1e9
+    hbm, peak_kind = peaks()
     # looping the single-system path: one handle per replica, stepped in turn
     # (replicas narrower than three search lengths on an axis have no
     # single-system cell grid and are left out of the loop)
@@ -639,6 +653,14 @@ def main_ensemble(args, ws, rank, local):
                                  "note": "one handle per replica with >= 3 cells per axis, calculate() in "
                                          "turn, host wall clock"},
         "speedup_vs_looped": value / loop_value,
+        "pair_interactions_per_s": {"fp32": ws * pairs * args.steps * mdn / (ms * 1e-3),
+                                    "pairs_within_cutoff_per_step": pairs},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "kernel": "ke_force_fp32 (kick + second half drift, all replicas)",
+                     "algorithmic_bytes_per_launch": force_bytes, "avg_launch_ms": avg_ms,
+                     "launches": flaunch, "peak_kind": peak_kind},
+        "gpu_launches": launches,
+        "clocks": clocks,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

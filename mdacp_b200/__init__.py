@@ -206,6 +206,9 @@ SIGNATURES = {
     "mdg_ensemble_rebuilds": (ctypes.c_int, [_H, _I64P, _I64P]),
     "mdg_ensemble_set_graph_mode": (ctypes.c_int, [_H, ctypes.c_int]),
     "mdg_ensemble_stream": (ctypes.c_void_p, [_H]),
+    "mdg_ensemble_set_kernel_timing": (ctypes.c_int, [_H, ctypes.c_int]),
+    "mdg_ensemble_kernel_time": (ctypes.c_int, [_H, _DP, _I64P, _I64P]),
+    "mdg_ensemble_list_stats": (ctypes.c_int, [_H, _I64P, _I64P]),
     "mdg_last_error": (ctypes.c_char_p, [_H]),
     "mdg_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "mdg_version": (ctypes.c_char_p, []),
@@ -564,6 +567,21 @@ class Ensemble:
 
     def stream(self):
         return self.lib.mdg_ensemble_stream(self.h)
+
+    def set_kernel_timing(self, on: bool):
+        self._check(self.lib.mdg_ensemble_set_kernel_timing(self.h, int(bool(on))))
+
+    def kernel_time(self):
+        """(force ms summed, force launches, kernels launched) since timing was set."""
+        ms, fl, kl = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.mdg_ensemble_kernel_time(self.h, ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(kl)))
+        return ms.value, fl.value, kl.value
+
+    def list_stats(self):
+        """(list entries of the current lists, unordered pairs within the cut-off)."""
+        le, pr = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.mdg_ensemble_list_stats(self.h, ctypes.byref(le), ctypes.byref(pr)))
+        return le.value, pr.value
 
     def states_by_id(self):
         """Per replica (q, v) ordered by upload index within the replica."""

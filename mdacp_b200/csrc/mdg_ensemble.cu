@@ -49,6 +49,7 @@ struct RepStatus {
   int disp, want_build, build, list_stale;
   int max_row, pad;
   long long total_images, rebuilds, steps, disp_checks;
+  long long list_entries;  // neighbour entries of the last build
 };
 
 struct Ens {
@@ -120,6 +121,26 @@ __device__ __forceinline__ void rep_max(unsigned long long *slot_base, size_t st
   }
 }
 
+// Sum of a count into the replica's slot, with the warp reduction of
+// rep_max for warps whose active lanes share one replica.  All lanes must call.
+__device__ __forceinline__ void rep_add(long long *slot_base, size_t stride_bytes, int r, long long v,
+                                        bool active) {
+  const int rr = active ? r : -1;
+  const int r0 = __shfl_sync(0xffffffffu, rr, 0);
+  const bool uniform = __all_sync(0xffffffffu, rr == r0) && r0 >= 0;
+  if (uniform) {
+    long long m = v;
+    for (int o = 16; o > 0; o >>= 1) m += __shfl_xor_sync(0xffffffffu, m, o);
+    if ((threadIdx.x & 31) == 0 && m) {
+      long long *p = (long long *)((char *)slot_base + stride_bytes * r0);
+      atomicAdd((unsigned long long *)p, (unsigned long long)m);
+    }
+  } else if (active && v) {
+    long long *p = (long long *)((char *)slot_base + stride_bytes * r);
+    atomicAdd((unsigned long long *)p, (unsigned long long)v);
+  }
+}
+
 // --------------------------------------------------------------- step kernels
 __global__ void ke_expiry(Ens e, cudaGraphConditionalHandle h_disp, int in_graph, int *flags) {
   __shared__ int any;
@@ -155,6 +176,7 @@ __global__ void ke_expiry(Ens e, cudaGraphConditionalHandle h_disp, int in_graph
   if (threadIdx.x == 0) {
     if (in_graph) cudaGraphSetConditional(h_disp, any);
     else flags[0] = any;
+    if (any) flags[2]++;  // steps that launch the skin-check branch
   }
 }
 
@@ -230,12 +252,14 @@ __global__ void ke_decide(Ens e, cudaGraphConditionalHandle h_build, int in_grap
       any = 1;
       st.max_row = 0;
       st.total_images = 0;
+      st.list_entries = 0;
     }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     if (in_graph) cudaGraphSetConditional(h_build, any);
     else flags[1] = any;
+    if (any) flags[3]++;  // steps that launch the rebuild branch
   }
 }
 
@@ -375,15 +399,13 @@ __global__ void __launch_bounds__(kEB) ke_copy_back(Ens e) {
   e.ids[s] = e.ids_tmp[s];
 }
 
-// The single-system list build per atom (same candidate order, same FP32
-// prefilter with the exact FP64 band); all-pairs with the minimum image for
-// small replicas.
-__global__ void __launch_bounds__(kEF) ke_build(Ens e) {
-  const int i = blockIdx.x * kEF + threadIdx.x;
-  if (i >= e.ntot || *e.error) return;
+// One atom's row of the list build, as the single-system build makes it
+// (same candidate order, same FP32 prefilter with the exact FP64 band);
+// all-pairs with the minimum image for small replicas.  Returns the entries
+// kept.
+__device__ __forceinline__ int ens_build_row(const Ens &e, int i) {
   const int r = e.rep_of[i];
   RepStatus &st = e.rs[r];
-  if (!st.build) return;
   const Rep rep = e.rep[r];
   const int maxnb = e.maxnb, stride = e.stride;
   int cnt = 0;
@@ -447,6 +469,15 @@ __global__ void __launch_bounds__(kEF) ke_build(Ens e) {
     for (int k = cnt; k < ((cnt + 3) & ~3); k++) e.nbr[(size_t)k * stride + i] = i;
   }
   atomicMax(&st.max_row, cnt);
+  return min(cnt, maxnb);
+}
+
+__global__ void __launch_bounds__(kEF) ke_build(Ens e) {
+  const int i = blockIdx.x * kEF + threadIdx.x;
+  const bool active = i < e.ntot && !*e.error && e.rs[e.rep_of[i]].build;
+  const int rr = active ? e.rep_of[i] : 0;
+  const int kept = active ? ens_build_row(e, i) : 0;
+  rep_add(&e.rs[0].list_entries, sizeof(RepStatus), rr, kept, active);
 }
 
 __global__ void ke_build_done(Ens e) {
@@ -635,6 +666,28 @@ __global__ void __launch_bounds__(kEB) ke_observe(Ens e) {
   atomicAdd(&e.sums[3 * r + 2], 0.5 * vir);
 }
 
+// Ordered pairs with r^2 <= rc^2 over the current lists (the FP64 pair
+// test of the force and observer kernels), summed over all replicas.
+__global__ void __launch_bounds__(kEB) ke_count_pairs(Ens e, unsigned long long *count) {
+  const int i = blockIdx.x * kEB + threadIdx.x;
+  int c = 0;
+  if (i < e.ntot) {
+    const Rep &rep = e.rep[e.rep_of[i]];
+    const double4 qi = e.q[i];
+    const int nn = e.nnbr[i];
+    for (int k = 0; k < nn; k++) {
+      const double4 qj = e.q[e.nbr[(size_t)k * e.stride + i]];
+      const double dx = dsub(image_of(qj.x, qi.x, rep.L[0], rep.hL[0]), qi.x);
+      const double dy = dsub(image_of(qj.y, qi.y, rep.L[1], rep.hL[1]), qi.y);
+      const double dz = dsub(image_of(qj.z, qi.z, rep.L[2], rep.hL[2]), qi.z);
+      const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+      c += r2 <= e.rc2;
+    }
+  }
+  const int w = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0 && w) atomicAdd(count, (unsigned long long)w);
+}
+
 __global__ void __launch_bounds__(kEB) ke_vmax_init(Ens e) {
   const int i = blockIdx.x * kEB + threadIdx.x;
   int r = 0;
@@ -666,6 +719,7 @@ struct mdg_ensemble {
   int *cell_rep = nullptr;
   int ncell_tot = 0;
   int *d_flags = nullptr;
+  unsigned long long *d_count = nullptr;  // ke_count_pairs
   cudaStream_t stream = nullptr, cap_stream = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool graph_dirty = true;
@@ -673,6 +727,11 @@ struct mdg_ensemble {
   bool state_set = false;
   int64_t kernel_launches = 0;
   int graph_kernels = 0;
+  // force-kernel timers (mdg_ensemble_set_kernel_timing)
+  bool timing = false;
+  std::vector<cudaEvent_t> ev;  // 2 per captured step
+  double force_ms = 0.0;
+  int64_t force_launches = 0;
 };
 
 namespace {
@@ -691,7 +750,7 @@ void e_free(mdg_ensemble *x) {
   Ens &e = x->e;
   void *ptrs[] = {(void *)e.rep, e.rs, (void *)e.rep_of, e.q, e.v, e.q_old, e.qfix, e.qloc, e.ids, e.cell,
                   e.cell_tmp, e.nbr, e.nnbr, e.cell_count, e.cell_start, e.slot, e.perm, e.perm2, e.q_tmp,
-                  e.v_tmp, e.ids_tmp, e.mult, e.cand, e.error, e.sums, x->cell_rep, x->d_flags};
+                  e.v_tmp, e.ids_tmp, e.mult, e.cand, e.error, e.sums, x->cell_rep, x->d_flags, x->d_count};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (x->exec) cudaGraphExecDestroy(x->exec);
@@ -718,19 +777,37 @@ void e_launch_build(mdg_ensemble *x, cudaStream_t s) {
   ke_build_done<<<1, 1024, 0, s>>>(e);
 }
 
-int e_launch_tail(mdg_ensemble *x, cudaStream_t s) {
+// The step after the skin decision; e0/e1 (optional) bracket the force
+// kernel.  Inside a stream capture an event record must be external to be
+// recorded when the graph runs (a plain record only orders the capture).
+int e_launch_tail(mdg_ensemble *x, cudaStream_t s, cudaEvent_t e0 = nullptr, cudaEvent_t e1 = nullptr,
+                  bool capture = false) {
   Ens &e = x->e;
+  auto rec = [&](cudaEvent_t ev) {
+    if (!ev) return;
+    if (capture) cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal);
+    else cudaEventRecord(ev, s);
+  };
   if (x->prm.precision == MDG_FP32_MIXED) {
     ke_drift<true><<<nb(e.ntot, kEB), kEB, 0, s>>>(e, 0);
+    rec(e0);
     ke_force_fp32<<<nb(e.ntot, kEF), kEF, 0, s>>>(e);
+    rec(e1);
     ke_step_done<<<1, 1024, 0, s>>>(e);
     return 3;
   }
   ke_drift<false><<<nb(e.ntot, kEB), kEB, 0, s>>>(e, 0);
+  rec(e0);
   ke_force_fp64<<<nb(e.ntot, kEF), kEF, 0, s>>>(e);
+  rec(e1);
   ke_drift<false><<<nb(e.ntot, kEB), kEB, 0, s>>>(e, 1);
   ke_step_done<<<1, 1024, 0, s>>>(e);
   return 4;
+}
+
+void e_destroy_events(mdg_ensemble *x) {
+  for (cudaEvent_t ev : x->ev) cudaEventDestroy(ev);
+  x->ev.clear();
 }
 
 struct ECapture {
@@ -775,6 +852,11 @@ cudaError_t e_add_if(ECapture &c, cudaGraphConditionalHandle hc, cudaGraph_t *bo
 mdg_status e_build_graph(mdg_ensemble *x) {
   if (x->exec) cudaGraphExecDestroy(x->exec);
   x->exec = nullptr;
+  e_destroy_events(x);
+  if (x->timing) {
+    x->ev.resize(2 * kEStepsPerGraph);
+    for (auto &ev : x->ev) ECUDA(cudaEventCreate(&ev));
+  }
   cudaGraph_t g;
   ECUDA(cudaGraphCreate(&g, 0));
   ECapture c{x->cap_stream, g, {}};
@@ -805,7 +887,8 @@ mdg_status e_build_graph(mdg_ensemble *x) {
       ECUDA(e_end(bc));
     }
     ECUDA(e_begin(c));
-    kernels += 2 + e_launch_tail(x, c.s);
+    kernels += 2 + e_launch_tail(x, c.s, x->timing ? x->ev[2 * s] : nullptr,
+                                 x->timing ? x->ev[2 * s + 1] : nullptr, true);
     ECUDA(e_end(c));
   }
   cudaError_t err = cudaGraphInstantiate(&x->exec, g, 0);
@@ -822,20 +905,29 @@ mdg_status e_step_eager(mdg_ensemble *x) {
   ECUDA(cudaMemcpyAsync(flags, x->d_flags, sizeof flags, cudaMemcpyDeviceToHost, x->stream));
   ECUDA(cudaStreamSynchronize(x->stream));
   x->kernel_launches++;
-  if (flags[0]) {
-    e_launch_disp(x, x->stream);
-    x->kernel_launches += 3;
-  }
+  if (flags[0]) e_launch_disp(x, x->stream);  // counted on the device (ke_expiry)
   ke_decide<<<1, 1024, 0, x->stream>>>(x->e, 0, 0, x->d_flags);
   ECUDA(cudaMemcpyAsync(flags, x->d_flags, sizeof flags, cudaMemcpyDeviceToHost, x->stream));
   ECUDA(cudaStreamSynchronize(x->stream));
   x->kernel_launches++;
-  if (flags[1]) {
-    e_launch_build(x, x->stream);
-    x->kernel_launches += 9;
+  if (flags[1]) e_launch_build(x, x->stream);  // counted on the device (ke_decide)
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (x->timing) {
+    ECUDA(cudaEventCreate(&e0));
+    ECUDA(cudaEventCreate(&e1));
   }
-  x->kernel_launches += e_launch_tail(x, x->stream);
+  x->kernel_launches += e_launch_tail(x, x->stream, e0, e1);
   ECUDA(cudaGetLastError());
+  if (x->timing) {
+    float ms = 0.f;
+    cudaError_t err = cudaEventSynchronize(e1);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ECUDA(err);
+    x->force_ms += ms;
+    x->force_launches++;
+  }
   return MDG_OK;
 }
 
@@ -1006,6 +1098,8 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
   if (err == cudaSuccess) err = edalloc(&e.sums, (size_t)3 * nrep);
   if (err == cudaSuccess) err = edalloc(&x->cell_rep, cells);
   if (err == cudaSuccess) err = edalloc(&x->d_flags, 4);
+  if (err == cudaSuccess) err = cudaMemsetAsync(x->d_flags, 0, 4 * sizeof(int), x->stream);
+  if (err == cudaSuccess) err = edalloc(&x->d_count, 1);
   if (err == cudaSuccess) {
     std::vector<int> rep_of(n, 0);
     for (int r = 0; r < nrep; r++)
@@ -1036,6 +1130,7 @@ mdg_status mdg_ensemble_destroy(mdg_ensemble *x) {
   cudaSetDevice(x->prm.device);
   cudaStreamSynchronize(x->stream);
   e_free(x);
+  e_destroy_events(x);
   if (x->cap_stream) cudaStreamDestroy(x->cap_stream);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;
@@ -1118,6 +1213,15 @@ mdg_status mdg_ensemble_calculate(mdg_ensemble *x, int nsteps) {
       ECUDA(cudaGraphLaunch(x->exec, x->stream));
       x->kernel_launches += x->graph_kernels;
       left -= kEStepsPerGraph;
+      if (x->timing) {
+        ECUDA(cudaStreamSynchronize(x->stream));
+        for (int s = 0; s < kEStepsPerGraph; s++) {
+          float ms = 0.f;
+          ECUDA(cudaEventElapsedTime(&ms, x->ev[2 * s], x->ev[2 * s + 1]));
+          x->force_ms += ms;
+          x->force_launches++;
+        }
+      }
     }
     while (left > 0) {
       if ((r = e_step_eager(x))) return r;
@@ -1185,6 +1289,60 @@ mdg_status mdg_ensemble_rebuilds(mdg_ensemble *x, int64_t *rebuilds, int64_t *st
 mdg_status mdg_ensemble_set_graph_mode(mdg_ensemble *x, int use_graphs) {
   if (!x) return MDG_ERR_INVALID_ARGUMENT;
   x->use_graphs = use_graphs != 0;
+  return MDG_OK;
+}
+
+mdg_status mdg_ensemble_set_kernel_timing(mdg_ensemble *x, int on) {
+  if (!x) return MDG_ERR_INVALID_ARGUMENT;
+  if ((on != 0) != x->timing) {
+    ECUDA(cudaStreamSynchronize(x->stream));
+    x->timing = on != 0;
+    x->graph_dirty = true;
+  }
+  x->force_ms = 0.0;
+  x->force_launches = 0;
+  x->kernel_launches = 0;
+  ECUDA(cudaMemsetAsync(x->d_flags + 2, 0, 2 * sizeof(int), x->stream));
+  ECUDA(cudaStreamSynchronize(x->stream));
+  return MDG_OK;
+}
+
+mdg_status mdg_ensemble_list_stats(mdg_ensemble *x, int64_t *list_entries, int64_t *pairs_within_cutoff) {
+  if (!x || !x->state_set) return MDG_ERR_STATE;
+  Ens &e = x->e;
+  std::vector<RepStatus> rs;
+  int err = 0;
+  mdg_status r = e_status(x, &err, &rs);
+  if (r) return r;
+  if (err) return e_translate(err);
+  long long entries = 0;
+  for (auto &st : rs) entries += st.list_entries;
+  if (list_entries) *list_entries = entries;
+  if (pairs_within_cutoff) {
+    unsigned long long h = 0;
+    ECUDA(cudaMemsetAsync(x->d_count, 0, sizeof(unsigned long long), x->stream));
+    ke_count_pairs<<<nb(e.ntot, kEB), kEB, 0, x->stream>>>(e, x->d_count);
+    ECUDA(cudaGetLastError());
+    ECUDA(cudaMemcpyAsync(&h, x->d_count, sizeof h, cudaMemcpyDeviceToHost, x->stream));
+    ECUDA(cudaStreamSynchronize(x->stream));
+    *pairs_within_cutoff = (int64_t)(h / 2);
+  }
+  return MDG_OK;
+}
+
+mdg_status mdg_ensemble_kernel_time(mdg_ensemble *x, double *force_ms, int64_t *force_launches,
+                                    int64_t *kernel_launches) {
+  if (!x) return MDG_ERR_INVALID_ARGUMENT;
+  if (force_ms) *force_ms = x->force_ms;
+  if (force_launches) *force_launches = x->force_launches;
+  if (kernel_launches) {
+    // the host counts the unconditional kernels; the branches taken (in
+    // graphs or eager steps) are counted on the device (3 and 9 kernels)
+    int branch[2] = {0, 0};
+    ECUDA(cudaMemcpyAsync(branch, x->d_flags + 2, sizeof branch, cudaMemcpyDeviceToHost, x->stream));
+    ECUDA(cudaStreamSynchronize(x->stream));
+    *kernel_launches = x->kernel_launches + 3ll * branch[0] + 9ll * branch[1];
+  }
   return MDG_OK;
 }
 

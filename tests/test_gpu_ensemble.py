@@ -78,3 +78,42 @@ def test_ensemble_rejects_box_below_two_search_lengths():
     with pytest.raises(M.MdgError) as e:
         M.Ensemble([(r.q, r.v, r.L)], cutoff=2.5)
     assert e.value.status == -7
+
+
+def _pairs_within_cutoff(q, L, rc):
+    d = q[:, None, :] - q[None, :, :]
+    d -= L * np.round(d / L)
+    r2 = (d * d).sum(-1)
+    iu = np.triu_indices(q.shape[0], 1)
+    return int((r2[iu] <= rc * rc).sum())
+
+
+def test_list_stats_and_kernel_counters():
+    # list entries: the sum of the single handles' lists after the same
+    # steps (the rebuild schedules are the same); pairs within the cut-off:
+    # a brute-force count on the host; the kernel counters agree between
+    # graph and eager stepping (the same skin decisions in both)
+    reps = replicas()[:3]
+    runs = []
+    for graphs in (True, False):
+        ens = M.Ensemble([(r.q, r.v, r.L) for r in reps], cutoff=2.5, time_step=0.005, precision=M.FP32_MIXED)
+        ens.set_graph_mode(graphs)
+        ens.set_kernel_timing(True)
+        ens.calculate(40)
+        fms, fl, kl = ens.kernel_time()
+        entries, pairs = ens.list_stats()
+        states = ens.states_by_id()
+        ens.close()
+        runs.append((fms, fl, kl, entries, pairs))
+    assert runs[0][1:] == runs[1][1:]
+    fms, fl, kl, entries, pairs = runs[0]
+    assert fl == 40 and fms > 0.0 and kl >= 40 * 5
+    want_entries = 0
+    for r in reps:
+        s = M.System(r.L, cutoff=2.5, time_step=0.005, capacity=r.n, precision=M.FP32_MIXED)
+        s.set_state(r.q, r.v)
+        s.calculate(40)
+        want_entries += s.info()["list_entries"]
+        s.close()
+    assert entries == want_entries
+    assert pairs == sum(_pairs_within_cutoff(q, np.asarray(r.L), 2.5) for (q, _), r in zip(states, reps))
