@@ -49,41 +49,46 @@ struct Pot {
   double eps, sigma, rc2;       // energy scale, length scale, cut-off^2 (absolute)
   double c0, c2;                // smoothed-LJ constants in units of sigma
   double a, b, w;               // shell of the smoothed pair count
+  // reciprocals and quotients of the above, formed once on the host
+  double inv_sigma, inv_w, inv_eps, eps_sigma, eps_sigma2;  // 1/sigma, 1/w, 1/eps, eps/sigma, eps/sigma^2
 };
 
 struct Grid {
   int ms[3];
-  double L[3], inv_cs[3];
-  const int *start;  // ncell + 1
-  const int *perm;   // atoms in cell order
+  double L[3], inv_cs[3], inv_L[3];
+  const int *start;   // ncell + 1
+  const int *perm;    // atoms in cell order
+  const double4 *qs;  // their positions in the same order (made with the grid)
 };
 
+// phi(s) and its first two derivatives; one division (1/s).
 __device__ __forceinline__ void phi_d(double s, const Pot &p, double &phi, double &d1, double &d2) {
-  const double is2 = 1.0 / (s * s);
+  const double is = 1.0 / s;
+  const double is2 = is * is;
   const double is6 = is2 * is2 * is2;
   const double is12 = is6 * is6;
   phi = 4.0 * (is12 - is6 + p.c2 * s * s + p.c0);
-  d1 = 4.0 * (-12.0 * is12 + 6.0 * is6 + 2.0 * p.c2 * s * s) / s;
+  d1 = 4.0 * (-12.0 * is12 + 6.0 * is6 + 2.0 * p.c2 * s * s) * is;
   d2 = 4.0 * (156.0 * is12 - 42.0 * is6 + 2.0 * p.c2 * s * s) * is2;
 }
 
 // U(r), U'(r), U''(r)
 __device__ __forceinline__ void pair_u(double r, const Pot &p, double &u, double &u1, double &u2) {
   double f, f1, f2;
-  phi_d(r / p.sigma, p, f, f1, f2);
+  phi_d(r * p.inv_sigma, p, f, f1, f2);
   u = p.eps * f;
-  u1 = p.eps / p.sigma * f1;
-  u2 = p.eps / (p.sigma * p.sigma) * f2;
+  u1 = p.eps_sigma * f1;
+  u2 = p.eps_sigma2 * f2;
 }
 
 __device__ __forceinline__ double logistic(double x) { return 1.0 / (1.0 + exp(-x)); }
 
 // smoothed shell count of one pair and its derivative in r
 __device__ __forceinline__ void shell(double r, const Pot &p, double &s, double &s1) {
-  const double x1 = (r - p.a) / p.w, x2 = (p.b - r) / p.w;
+  const double x1 = (r - p.a) * p.inv_w, x2 = (p.b - r) * p.inv_w;
   const double g1 = logistic(x1), g2 = logistic(x2);
   s = g1 * g2;
-  s1 = (g1 * (1.0 - g1) * g2 - g1 * g2 * (1.0 - g2)) / p.w;
+  s1 = (g1 * (1.0 - g1) * g2 - g1 * g2 * (1.0 - g2)) * p.inv_w;
 }
 
 __device__ __forceinline__ int cell_axis(double x, double L, double inv_cs, int ms) {
@@ -100,7 +105,8 @@ __device__ __forceinline__ int cell_of(const double4 &q, const Grid &g) {
 }
 
 // Calls f(j, d, r) for every partner j != i with r < r_c, d = minimum image of
-// q_i - q_j, over the 27 cells around i's, each in index order.  TPA lanes
+// q_i - q_j, over the 27 cells around i's, each in index order (partner
+// positions read from the grid's cell-ordered copy).  TPA lanes
 // share one atom: lane `sub` takes cells sub, sub + TPA, ... of the 27 (the
 // caller combines the lanes' sums with group_sum).
 template <int TPA, class F>
@@ -117,9 +123,9 @@ __device__ __forceinline__ void for_pairs(const double4 *q, const Grid &g, const
     for (int k = g.start[c]; k < g.start[c + 1]; k++) {
       const int j = g.perm[k];
       if (j == i) continue;
-      const double4 qj = q[j];
+      const double4 qj = g.qs[k];
       double d[3] = {qi.x - qj.x, qi.y - qj.y, qi.z - qj.z};
-      for (int a = 0; a < 3; a++) d[a] -= g.L[a] * rint(d[a] / g.L[a]);
+      for (int a = 0; a < 3; a++) d[a] -= g.L[a] * rint(d[a] * g.inv_L[a]);
       const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
       if (r2 < p.rc2) f(j, d, sqrt(r2));
     }
@@ -194,20 +200,30 @@ __global__ void a_fill(int n, const int *cell, const int *start, int *fill, int 
   perm[start[c] + atomicAdd(&fill[c], 1)] = i;
 }
 
-// order every cell by atom index (insertion sort, thread per cell)
-__global__ void a_sort(int ncell, const int *start, int *perm) {
-  const int c = blockIdx.x * kAB + threadIdx.x;
+// Orders every cell by atom index, one warp per cell: each entry's new
+// place is the count of smaller indices in the cell (indices are distinct).
+// perm_in is the fill order, perm_out the sorted one.
+__global__ void a_sort(int ncell, const int *start, const int *perm_in, int *perm_out) {
+  const int c = (blockIdx.x * kAB + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (c >= ncell) return;
-  const int b = start[c], e = start[c + 1];
-  for (int k = b + 1; k < e; k++) {
-    const int x = perm[k];
-    int m = k - 1;
-    while (m >= b && perm[m] > x) {
-      perm[m + 1] = perm[m];
-      m--;
+  const int b = start[c], cnt = start[c + 1] - b;
+  for (int base = 0; base < cnt; base += 32) {
+    const int me = base + lane;
+    const int key = me < cnt ? perm_in[b + me] : 0x7fffffff;
+    int rank = 0;
+    for (int ob = 0; ob < cnt; ob += 32) {
+      const int okey = ob + lane < cnt ? perm_in[b + ob + lane] : 0x7fffffff;
+      for (int k = 0; k < 32; k++) rank += (ob + k < cnt) && (__shfl_sync(0xffffffffu, okey, k) < key);
     }
-    perm[m + 1] = x;
+    if (me < cnt) perm_out[b + rank] = key;
   }
+}
+
+// Positions in cell order for the pair kernels.
+__global__ void a_gather(const double4 *x, const int *perm, double4 *xs, int n) {
+  const int k = blockIdx.x * kAB + threadIdx.x;
+  if (k < n) xs[k] = x[perm[k]];
 }
 
 // --------------------------------------------------------------- physics
@@ -248,7 +264,7 @@ __global__ void __launch_bounds__(kAB) a_loss(const double4 *q, int n, Grid g, P
       shell(r, p, s, s1);
       v[0] += 0.5 * u;
       v[1] += 0.5 * s;
-      v[2] += 0.5 * (-(r / p.sigma) * u1);  // dU/dsigma at fixed r
+      v[2] += 0.5 * (-(r * p.inv_sigma) * u1);  // dU/dsigma at fixed r
       const double c = (u1 + s1) / r;
       gx += c * d[0];
       gy += c * d[1];
@@ -285,18 +301,19 @@ __global__ void __launch_bounds__(kAB) a_hvp(const double4 *q, int n, Grid g, Po
       double uu, u1, u2;
       pair_u(r, p, uu, u1, u2);
       const double4 uj = u[j];
-      const double ex = d[0] / r, ey = d[1] / r, ez = d[2] / r;
+      const double ir = 1.0 / r;
+      const double ex = d[0] * ir, ey = d[1] * ir, ez = d[2] * ir;
       const double dux = ui.x - uj.x, duy = ui.y - uj.y, duz = ui.z - uj.z;
       const double proj = ex * dux + ey * duy + ez * duz;
-      const double t = u1 / r;
+      const double t = u1 * ir;
       // K du = U'' e (e.du) + U'/r (du - e (e.du))
       wx += u2 * ex * proj + t * (dux - ex * proj);
       wy += u2 * ey * proj + t * (duy - ey * proj);
       wz += u2 * ez * proj + t * (duz - ez * proj);
       // F_i = sum_j -U'(r) e: dF_i/deps = -(U'/eps) e, dF_i/dsigma = (U' + r U'')/sigma e
       const double eu = ex * ui.x + ey * ui.y + ez * ui.z;
-      v[0] += -(u1 / p.eps) * eu;
-      v[1] += (u1 + r * u2) / p.sigma * eu;
+      v[0] += -(u1 * p.inv_eps) * eu;
+      v[1] += (u1 + r * u2) * p.inv_sigma * eu;
     });
   }
   wx = group_sum<TPA>(wx);
@@ -306,13 +323,25 @@ __global__ void __launch_bounds__(kAB) a_hvp(const double4 *q, int n, Grid g, Po
   block_sums<2>(v, part);
 }
 
-// Fixed-order sum of nb blocks' NS partials into out[k] (one warp); the
-// per-step sums stay on the device until the end of the run.
-__global__ void a_reduce(const double *part, int nb, int ns, double *out) {
-  if (threadIdx.x >= ns) return;
-  double x = 0.0;
-  for (int b = 0; b < nb; b++) x += part[(size_t)b * ns + threadIdx.x];
-  out[threadIdx.x] = x;
+// Fixed-order sum of nb blocks' ns (<= 3) partials into out[k], one block of
+// kRB threads: thread t sums blocks t, t + kRB, ... in order, then a fixed
+// tree; the per-step sums stay on the device until the end of the run.
+constexpr int kRB = 256;
+__global__ void __launch_bounds__(kRB) a_reduce(const double *part, int nb, int ns, double *out) {
+  __shared__ double sm[3][kRB];
+  const int t = threadIdx.x;
+  for (int k = 0; k < ns; k++) {
+    double x = 0.0;
+    for (int b = t; b < nb; b += kRB) x += part[(size_t)b * ns + k];
+    sm[k][t] = x;
+  }
+  __syncthreads();
+  for (int o = kRB / 2; o > 0; o >>= 1) {
+    if (t < o)
+      for (int k = 0; k < ns; k++) sm[k][t] += sm[k][t + o];
+    __syncthreads();
+  }
+  if (t < ns) out[t] = sm[t][0];
 }
 
 // --------------------------------------------------------- integration
@@ -380,7 +409,8 @@ struct Run {
   double4 *lq = nullptr, *lv = nullptr, *u = nullptr, *w = nullptr;
   double4 *ck_q = nullptr, *ck_v = nullptr;    // checkpoints
   double4 *seg_qh = nullptr, *seg_v = nullptr;  // one segment's q_h and v'
-  int *cell = nullptr, *count = nullptr, *start = nullptr, *fill = nullptr, *perm = nullptr;
+  int *cell = nullptr, *count = nullptr, *start = nullptr, *fill = nullptr, *perm = nullptr, *perm_fill = nullptr;
+  double4 *qs = nullptr;                        // positions in cell order
   double *part = nullptr;                       // block partials of the pair kernels
   double *loss_sums = nullptr;                  // per step: PE, S, dPE/dsigma
   double *adj_sums = nullptr;                   // per reverse step: u . dF/d(eps, sigma)
@@ -404,8 +434,9 @@ struct Run {
     cudaMemsetAsync(fill, 0, sizeof(int) * ncell, s);
     a_count<<<nblk(n), kAB, 0, s>>>(x, n, g, cell, count);
     a_scan<<<1, 1024, 0, s>>>(count, start, ncell);
-    a_fill<<<nblk(n), kAB, 0, s>>>(n, cell, start, fill, perm);
-    a_sort<<<nblk(ncell), kAB, 0, s>>>(ncell, start, perm);
+    a_fill<<<nblk(n), kAB, 0, s>>>(n, cell, start, fill, perm_fill);
+    a_sort<<<nblk(ncell * 32), kAB, 0, s>>>(ncell, start, perm_fill, perm);
+    a_gather<<<nblk(n), kAB, 0, s>>>(x, perm, qs, n);
   }
   void force(const double4 *x) {
     const int nb = pair_blocks();
@@ -448,7 +479,7 @@ struct Run {
   void loss_at(const double4 *x, double scale, double *out) {
     cells(x);
     loss(x, scale != 0.0 ? lq : nullptr, scale);
-    if (out) a_reduce<<<1, 32, 0, s>>>(part, pair_blocks(), 3, out);
+    if (out) a_reduce<<<1, kRB, 0, s>>>(part, pair_blocks(), 3, out);
   }
 };
 
@@ -539,6 +570,7 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
     if (R.g.ms[d] < 3) return MDG_ERR_BOX_TOO_SMALL;
     R.g.L[d] = L;
     R.g.inv_cs[d] = R.g.ms[d] / L;
+    R.g.inv_L[d] = 1.0 / L;
   }
   R.ncell = R.g.ms[0] * R.g.ms[1] * R.g.ms[2];
   const double sc = prm->cutoff;
@@ -550,6 +582,11 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   R.p.a = prm->shell_lo;
   R.p.b = prm->shell_hi;
   R.p.w = prm->shell_width;
+  R.p.inv_sigma = 1.0 / R.p.sigma;
+  R.p.inv_w = 1.0 / R.p.w;
+  R.p.inv_eps = 1.0 / R.p.eps;
+  R.p.eps_sigma = R.p.eps / R.p.sigma;
+  R.p.eps_sigma2 = R.p.eps / (R.p.sigma * R.p.sigma);
   const int T = prm->steps, k = prm->checkpoint_every;
   const int nck = (T + k - 1) / k + 1;
   const size_t max_blocks = ((size_t)n * 8 + kAB - 1) / kAB;
@@ -564,6 +601,8 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   if (e == cudaSuccess) e = R.alloc(&R.fill, R.ncell);
   if (e == cudaSuccess) e = R.alloc(&R.start, R.ncell + 1);
   if (e == cudaSuccess) e = R.alloc(&R.perm, n);
+  if (e == cudaSuccess) e = R.alloc(&R.perm_fill, n);
+  if (e == cudaSuccess) e = R.alloc(&R.qs, n);
   if (e == cudaSuccess) e = R.alloc(&R.part, max_blocks * 3);
   if (e == cudaSuccess) e = R.alloc(&R.loss_sums, (size_t)T * 3);
   if (grad) {
@@ -580,6 +619,7 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? MDG_ERR_CAPACITY : MDG_ERR_CUDA;
   R.g.start = R.start;
   R.g.perm = R.perm;
+  R.g.qs = R.qs;
 
   // upload (n x 3 host arrays -> double4)
   {
@@ -638,7 +678,7 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
       a_rev1<<<nblk(n), kAB, 0, R.s>>>(R.lq, R.lv, R.u, n, R.dt);
       R.cells(qh);
       R.hvp(qh);
-      a_reduce<<<1, 32, 0, R.s>>>(R.part, R.pair_blocks(), 2, R.adj_sums + (size_t)2 * t);
+      a_reduce<<<1, kRB, 0, R.s>>>(R.part, R.pair_blocks(), 2, R.adj_sums + (size_t)2 * t);
       a_rev2<<<nblk(n), kAB, 0, R.s>>>(R.lq, R.lv, R.w, n, R.dt);
     }
   }
