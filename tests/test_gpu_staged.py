@@ -87,6 +87,26 @@ def test_rows_grow_with_staging():
     assert a.info()["max_neighbors"] >= a.info()["max_row"]
 
 
+def test_staged_after_change_scale_and_restart(tmp_path):
+    # a new cell grid (ChangeScale) and a checkpoint restart both rebuild the
+    # list, and with it the stage plans
+    st = W.fcc_liquid(12, 0.8442, 1.0, seed=78, jitter=0.05, rc=2.5, dt=0.005)
+    a, b = pair_of(st, -1)
+    for s in (a, b):
+        s.calculate(20)
+        s.change_scale(1.04)
+        s.calculate(25)
+    assert_same(a, b)
+    a.save_checkpoint(tmp_path / "staged.ckpt")
+    c = M.System(a.params.L, cutoff=st.rc, time_step=st.dt, capacity=st.n, precision=M.FP32_MIXED,
+                 stage_atoms=-1)
+    c.load_checkpoint(tmp_path / "staged.ckpt")
+    for s in (a, b, c):
+        s.calculate(30)
+    assert_same(a, b)
+    assert_same(a, c)
+
+
 def test_stage_size_is_checked():
     st = W.fcc_liquid(5, 0.8442, 1.0, seed=77, rc=2.5)
     for bad in (-2, 12289):
