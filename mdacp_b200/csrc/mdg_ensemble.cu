@@ -52,6 +52,17 @@ struct RepStatus {
   long long list_entries;  // neighbour entries of the last build
 };
 
+// The replicas a skin check or a rebuild acts on, compacted in replica order
+// (ke_make_list), with the prefix sums that map a work index to an atom or
+// a cell: the per-atom and per-cell kernels of those branches sweep only
+// these atoms and cells.
+struct WorkList {
+  int *rep;          // [count[0]] acting replicas, ascending
+  int *atom_prefix;  // [count[0] + 1] first work atom of each
+  int *cell_prefix;  // [count[0] + 1] first work cell of each
+  int *count;        // replicas, atoms, cells
+};
+
 struct Ens {
   const Rep *rep;
   RepStatus *rs;
@@ -67,6 +78,7 @@ struct Ens {
   int2 *cand;  // nrep x cll candidate copies (slot, image code)
   int *error;
   double *sums;  // nrep x 3 observer sums
+  WorkList wd, wb;  // skin-check and rebuild work lists
   int stride, maxnb, nrep, ntot, cll;
   double rc2, sl, sl2, c0, c2, dt, buffer_length;
   float rc2f, c2x8f, sl2_lo, sl2_hi;
@@ -141,6 +153,69 @@ __device__ __forceinline__ void rep_add(long long *slot_base, size_t stride_byte
   }
 }
 
+// Index k of the work-list replica that holds work item g (the largest k
+// with prefix[k] <= g; nk >= 1).
+__device__ __forceinline__ int work_find(const int *prefix, int nk, int g) {
+  int lo = 0, hi = nk - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (prefix[mid] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Replica and atom slot of work atom g of list w.
+__device__ __forceinline__ int work_atom(const Ens &e, const WorkList &w, int g, int *r) {
+  const int k = work_find(w.atom_prefix, w.count[0], g);
+  *r = w.rep[k];
+  return e.rep[*r].atom_off + (g - w.atom_prefix[k]);
+}
+
+// One block, 1024 threads: the work list of the replicas whose disp (WHICH
+// 0) or build (WHICH 1) flag is set.
+template <int WHICH>
+__global__ void __launch_bounds__(1024) ke_make_list(Ens e) {
+  const WorkList w = WHICH ? e.wb : e.wd;
+  __shared__ int base_k, base_a, base_c, tk, ta, tc;
+  if (threadIdx.x == 0) base_k = base_a = base_c = 0;
+  __syncthreads();
+  for (int r0 = 0; r0 < e.nrep; r0 += 1024) {
+    const int r = r0 + threadIdx.x;
+    int f = 0, na = 0, nc = 0;
+    if (r < e.nrep) {
+      f = WHICH ? e.rs[r].build : e.rs[r].disp;
+      f = f != 0;
+      if (f) {
+        na = e.rep[r].n;
+        nc = e.rep[r].ncell;
+      }
+    }
+    const int k = block_exclusive_scan<1024>(f, &tk);
+    const int a = block_exclusive_scan<1024>(na, &ta);
+    const int c = block_exclusive_scan<1024>(nc, &tc);
+    if (f) {
+      w.rep[base_k + k] = r;
+      w.atom_prefix[base_k + k] = base_a + a;
+      w.cell_prefix[base_k + k] = base_c + c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      base_k += tk;
+      base_a += ta;
+      base_c += tc;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    w.atom_prefix[base_k] = base_a;
+    w.cell_prefix[base_k] = base_c;
+    w.count[0] = base_k;
+    w.count[1] = base_a;
+    w.count[2] = base_c;
+  }
+}
+
 // --------------------------------------------------------------- step kernels
 __global__ void ke_expiry(Ens e, cudaGraphConditionalHandle h_disp, int in_graph, int *flags) {
   __shared__ int any;
@@ -183,36 +258,39 @@ __global__ void ke_expiry(Ens e, cudaGraphConditionalHandle h_disp, int in_graph
 __device__ __forceinline__ CopyView ens_view(const Ens &e) { return CopyView{e.q_old, e.q, e.v, e.mult}; }
 
 // Skin check per replica, over the reference's copies (see for_each_copy).
+// (The atoms of the checked replicas, through the skin-check work list;
+// block-uniform sweeps, so every lane reaches rep_max.)
 __global__ void __launch_bounds__(kEB) ke_disp_max(Ens e) {
-  const int i = blockIdx.x * kEB + threadIdx.x;
-  int r = 0;
-  double d2 = 0.0;
-  bool active = false;
-  if (i < e.ntot) {
-    r = e.rep_of[i];
-    if (e.rs[r].disp) {
+  const int total = e.wd.count[1];
+  for (int base = blockIdx.x * kEB; base < total; base += gridDim.x * kEB) {
+    const int g = base + threadIdx.x;
+    const bool active = g < total;
+    int r = 0;
+    double d2 = 0.0;
+    if (active) {
+      const int i = work_atom(e, e.wd, g, &r);
       for_each_copy(ens_view(e), e.rep[r].L, i, e.lag, [&](int, double x) { d2 = fmax(d2, x); });
-      active = true;
     }
+    rep_max(&e.rs[0].dr2max_bits, sizeof(RepStatus), r, d2, active);
   }
-  rep_max(&e.rs[0].dr2max_bits, sizeof(RepStatus), r, d2, active);
 }
 
 __global__ void __launch_bounds__(kEB) ke_disp_collect(Ens e) {
-  const int i = blockIdx.x * kEB + threadIdx.x;
-  if (i >= e.ntot) return;
-  const int r = e.rep_of[i];
-  RepStatus &st = e.rs[r];
-  if (!st.disp) return;
-  const double c = e.buffer_length - sqrt(__longlong_as_double((long long)st.dr2max_bits));
-  const double c_d2 = c * c;
-  for_each_copy(ens_view(e), e.rep[r].L, i, e.lag, [&](int code, double d2) {
-    if (d2 > c_d2) {
-      atomicAdd(&st.cand_weighted, 1);
-      const int k = atomicAdd(&st.cand_n, 1);
-      if (k < e.cll) e.cand[(size_t)r * e.cll + k] = make_int2(i, code);
-    }
-  });
+  const int total = e.wd.count[1];
+  for (int g = blockIdx.x * kEB + threadIdx.x; g < total; g += gridDim.x * kEB) {
+    int r;
+    const int i = work_atom(e, e.wd, g, &r);
+    RepStatus &st = e.rs[r];
+    const double c = e.buffer_length - sqrt(__longlong_as_double((long long)st.dr2max_bits));
+    const double c_d2 = c * c;
+    for_each_copy(ens_view(e), e.rep[r].L, i, e.lag, [&](int code, double d2) {
+      if (d2 > c_d2) {
+        atomicAdd(&st.cand_weighted, 1);
+        const int k = atomicAdd(&st.cand_n, 1);
+        if (k < e.cll) e.cand[(size_t)r * e.cll + k] = make_int2(i, code);
+      }
+    });
+  }
 }
 
 // kEPairParts blocks per replica (blockIdx.y) share the rows of the
@@ -271,12 +349,10 @@ __global__ void __launch_bounds__(kEB) ke_clear_cells(Ens e) {
   for (int c = threadIdx.x; c < rep.ncell; c += kEB) e.cell_count[rep.cell_off + c] = 0;
 }
 
-__global__ void __launch_bounds__(kEB) ke_cell_assign(Ens e) {
-  const int i = blockIdx.x * kEB + threadIdx.x;
-  if (i >= e.ntot || *e.error) return;
-  const int r = e.rep_of[i];
-  if (!e.rs[r].build) return;
-  const Rep rep = e.rep[r];
+// Wraps atom i of replica r into its box (Variables::AdjustPeriodicBoundary,
+// src/variables.cc:63-84), checks it, and files it in its cell.
+__device__ __forceinline__ void cell_assign_atom(const Ens &e, int r, int i) {
+  const Rep &rep = e.rep[r];
   double4 q = e.q[i];
   double x[3] = {q.x, q.y, q.z};
   int cc[3];
@@ -300,6 +376,17 @@ __global__ void __launch_bounds__(kEB) ke_cell_assign(Ens e) {
   const int c = rep.cell_off + (cc[2] * rep.ms[1] + cc[1]) * rep.ms[0] + cc[0];
   e.cell[i] = c;
   e.slot[i] = atomicAdd(&e.cell_count[c], 1);
+}
+
+// Atoms of the rebuilding replicas (rebuild work list) from here to ke_build.
+__global__ void __launch_bounds__(kEB) ke_cell_assign(Ens e) {
+  if (*e.error) return;
+  const int total = e.wb.count[1];
+  for (int g = blockIdx.x * kEB + threadIdx.x; g < total; g += gridDim.x * kEB) {
+    int r;
+    const int i = work_atom(e, e.wb, g, &r);
+    cell_assign_atom(e, r, i);
+  }
 }
 
 // One block per rebuilding replica: exclusive scan of its cells, offset by
@@ -330,20 +417,19 @@ __global__ void __launch_bounds__(kEB) ke_scan_cells(Ens e) {
 }
 
 __global__ void __launch_bounds__(kEB) ke_scatter(Ens e) {
-  const int i = blockIdx.x * kEB + threadIdx.x;
-  if (i >= e.ntot || *e.error) return;
-  if (!e.rs[e.rep_of[i]].build) return;
-  e.perm[e.cell_start[e.cell[i]] + e.slot[i]] = i;
+  if (*e.error) return;
+  const int total = e.wb.count[1];
+  for (int g = blockIdx.x * kEB + threadIdx.x; g < total; g += gridDim.x * kEB) {
+    int r;
+    const int i = work_atom(e, e.wb, g, &r);
+    e.perm[e.cell_start[e.cell[i]] + e.slot[i]] = i;
+  }
 }
 
-// Warp per cell of a rebuilding replica: order by upload id.  cell_rep maps
-// a global cell to its replica.
-__global__ void ke_sort_cells(Ens e, const int *cell_rep, int ncell_tot) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= ncell_tot || *e.error) return;
-  if (!e.rs[cell_rep[warp]].build) return;
-  const int beg = e.cell_start[warp], cnt = e.cell_start[warp + 1] - beg;
+// Warp per cell of a rebuilding replica (the cells of the rebuild work
+// list): order by upload id.
+__device__ __forceinline__ void sort_cell(const Ens &e, int cell, int lane) {
+  const int beg = e.cell_start[cell], cnt = e.cell_start[cell + 1] - beg;
   for (int base = 0; base < cnt; base += 32) {
     const int me = base + lane;
     int my_slot = -1, my_key = 0x7fffffff;
@@ -365,11 +451,21 @@ __global__ void ke_sort_cells(Ens e, const int *cell_rep, int ncell_tot) {
   }
 }
 
-__global__ void __launch_bounds__(kEB) ke_permute(Ens e) {
-  const int s = blockIdx.x * kEB + threadIdx.x;
-  if (s >= e.ntot || *e.error) return;
-  const int r = e.rep_of[s];
-  if (!e.rs[r].build) return;
+__global__ void __launch_bounds__(kEB) ke_sort_cells(Ens e) {
+  if (*e.error) return;
+  const int total = e.wb.count[2], nk = e.wb.count[0];
+  const int lane = threadIdx.x & 31;
+  const int wstride = gridDim.x * (kEB / 32);
+  for (int gc = blockIdx.x * (kEB / 32) + (threadIdx.x >> 5); gc < total; gc += wstride) {
+    const int k = work_find(e.wb.cell_prefix, nk, gc);
+    sort_cell(e, e.rep[e.wb.rep[k]].cell_off + (gc - e.wb.cell_prefix[k]), lane);
+  }
+}
+
+// Gathers the atom that goes to slot s of replica r into the temporary
+// arrays, snapshots q_old (PairList::Init), its ghost-strip membership and
+// cell-local coordinates; returns its copy count (atom + ghost images).
+__device__ __forceinline__ int permute_atom(const Ens &e, int r, int s) {
   const Rep rep = e.rep[r];
   const Box b = box_of(e, rep);
   const int o = e.perm2[s];
@@ -387,16 +483,34 @@ __global__ void __launch_bounds__(kEB) ke_permute(Ens e) {
   const int cx = c % rep.ms[0], cy = (c / rep.ms[0]) % rep.ms[1], cz = c / (rep.ms[0] * rep.ms[1]);
   e.qloc[s] = make_float4((float)(q.x - cx * rep.cs[0]), (float)(q.y - cy * rep.cs[1]),
                           (float)(q.z - cz * rep.cs[2]), 0.f);
-  atomicAdd((unsigned long long *)&e.rs[r].total_images, (unsigned long long)m);
+  return m;
+}
+
+__global__ void __launch_bounds__(kEB) ke_permute(Ens e) {
+  const bool err = *e.error != 0;
+  const int total = e.wb.count[1];
+  for (int base = blockIdx.x * kEB; base < total; base += gridDim.x * kEB) {
+    const int g = base + threadIdx.x;
+    const bool active = g < total && !err;
+    int r = 0, m = 0;
+    if (active) {
+      const int s = work_atom(e, e.wb, g, &r);
+      m = permute_atom(e, r, s);
+    }
+    rep_add(&e.rs[0].total_images, sizeof(RepStatus), r, m, active);
+  }
 }
 
 __global__ void __launch_bounds__(kEB) ke_copy_back(Ens e) {
-  const int s = blockIdx.x * kEB + threadIdx.x;
-  if (s >= e.ntot || *e.error) return;
-  if (!e.rs[e.rep_of[s]].build) return;
-  e.q[s] = e.q_tmp[s];
-  e.v[s] = e.v_tmp[s];
-  e.ids[s] = e.ids_tmp[s];
+  if (*e.error) return;
+  const int total = e.wb.count[1];
+  for (int g = blockIdx.x * kEB + threadIdx.x; g < total; g += gridDim.x * kEB) {
+    int r;
+    const int s = work_atom(e, e.wb, g, &r);
+    e.q[s] = e.q_tmp[s];
+    e.v[s] = e.v_tmp[s];
+    e.ids[s] = e.ids_tmp[s];
+  }
 }
 
 // One atom's row of the list build, as the single-system build makes it
@@ -473,11 +587,14 @@ __device__ __forceinline__ int ens_build_row(const Ens &e, int i) {
 }
 
 __global__ void __launch_bounds__(kEF) ke_build(Ens e) {
-  const int i = blockIdx.x * kEF + threadIdx.x;
-  const bool active = i < e.ntot && !*e.error && e.rs[e.rep_of[i]].build;
-  const int rr = active ? e.rep_of[i] : 0;
-  const int kept = active ? ens_build_row(e, i) : 0;
-  rep_add(&e.rs[0].list_entries, sizeof(RepStatus), rr, kept, active);
+  const int total = e.wb.count[1];
+  for (int base = blockIdx.x * kEF; base < total; base += gridDim.x * kEF) {
+    const int g = base + threadIdx.x;
+    const bool active = g < total && !*e.error;
+    int r = 0, kept = 0;
+    if (active) kept = ens_build_row(e, work_atom(e, e.wb, g, &r));
+    rep_add(&e.rs[0].list_entries, sizeof(RepStatus), r, kept, active);
+  }
 }
 
 __global__ void ke_build_done(Ens e) {
@@ -716,10 +833,11 @@ struct mdg_ensemble {
   mdg_params prm{};
   Ens e{};
   std::vector<Rep> reps;
-  int *cell_rep = nullptr;
   int ncell_tot = 0;
   int *d_flags = nullptr;
   unsigned long long *d_count = nullptr;  // ke_count_pairs
+  int *d_lists = nullptr;                 // storage of the two work lists
+  int work_blocks = 0;                    // grid of the work-list sweeps
   cudaStream_t stream = nullptr, cap_stream = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool graph_dirty = true;
@@ -750,30 +868,42 @@ void e_free(mdg_ensemble *x) {
   Ens &e = x->e;
   void *ptrs[] = {(void *)e.rep, e.rs, (void *)e.rep_of, e.q, e.v, e.q_old, e.qfix, e.qloc, e.ids, e.cell,
                   e.cell_tmp, e.nbr, e.nnbr, e.cell_count, e.cell_start, e.slot, e.perm, e.perm2, e.q_tmp,
-                  e.v_tmp, e.ids_tmp, e.mult, e.cand, e.error, e.sums, x->cell_rep, x->d_flags, x->d_count};
+                  e.v_tmp, e.ids_tmp, e.mult, e.cand, e.error, e.sums, x->d_flags, x->d_count,
+                  x->d_lists};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (x->exec) cudaGraphExecDestroy(x->exec);
   x->exec = nullptr;
 }
 
+// Kernels launched by one skin-check and one rebuild branch.
+constexpr int kEDispKernels = 4, kEBuildKernels = 10;
+
+// The per-atom and per-cell kernels of the branches sweep the work list with
+// a grid of at most x->work_blocks blocks (full occupancy of every SM).
 void e_launch_disp(mdg_ensemble *x, cudaStream_t s) {
   Ens &e = x->e;
-  ke_disp_max<<<nb(e.ntot, kEB), kEB, 0, s>>>(e);
-  ke_disp_collect<<<nb(e.ntot, kEB), kEB, 0, s>>>(e);
+  const int gb = std::min(nb(e.ntot, kEB), x->work_blocks);
+  ke_make_list<0><<<1, 1024, 0, s>>>(e);
+  ke_disp_max<<<gb, kEB, 0, s>>>(e);
+  ke_disp_collect<<<gb, kEB, 0, s>>>(e);
   ke_disp_pairs<<<dim3(e.nrep, kEPairParts), 256, 0, s>>>(e);
 }
 
 void e_launch_build(mdg_ensemble *x, cudaStream_t s) {
   Ens &e = x->e;
+  const int gb = std::min(nb(e.ntot, kEB), x->work_blocks);
+  const int gf = std::min(nb(e.ntot, kEF), 2 * x->work_blocks);
+  const int gc = std::min(nb(x->ncell_tot * 32, kEB), x->work_blocks);
+  ke_make_list<1><<<1, 1024, 0, s>>>(e);
   ke_clear_cells<<<e.nrep, kEB, 0, s>>>(e);
-  ke_cell_assign<<<nb(e.ntot, kEB), kEB, 0, s>>>(e);
+  ke_cell_assign<<<gb, kEB, 0, s>>>(e);
   ke_scan_cells<<<e.nrep, kEB, 0, s>>>(e);
-  ke_scatter<<<nb(e.ntot, kEB), kEB, 0, s>>>(e);
-  ke_sort_cells<<<nb(x->ncell_tot * 32, kEB), kEB, 0, s>>>(e, x->cell_rep, x->ncell_tot);
-  ke_permute<<<nb(e.ntot, kEB), kEB, 0, s>>>(e);
-  ke_copy_back<<<nb(e.ntot, kEB), kEB, 0, s>>>(e);
-  ke_build<<<nb(e.ntot, kEF), kEF, 0, s>>>(e);
+  ke_scatter<<<gb, kEB, 0, s>>>(e);
+  ke_sort_cells<<<gc, kEB, 0, s>>>(e);
+  ke_permute<<<gb, kEB, 0, s>>>(e);
+  ke_copy_back<<<gb, kEB, 0, s>>>(e);
+  ke_build<<<gf, kEF, 0, s>>>(e);
   ke_build_done<<<1, 1024, 0, s>>>(e);
 }
 
@@ -1003,7 +1133,6 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
   x->reps.resize(nrep);
   long long atoms = 0;
   int cells = 0;
-  std::vector<int> cell_rep;
   for (int r = 0; r < nrep; r++) {
     Rep &rp = x->reps[r];
     memset(&rp, 0, sizeof rp);
@@ -1035,7 +1164,6 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
     rp.cell_off = cells;
     rp.atom_off = (int)atoms;
     rp.n = replicas[r].n;
-    for (int c = 0; c < rp.ncell; c++) cell_rep.push_back(r);
     cells += rp.ncell;
     atoms += replicas[r].n;
   }
@@ -1096,18 +1224,34 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
   if (err == cudaSuccess) err = edalloc(&e.cand, (size_t)nrep * e.cll);
   if (err == cudaSuccess) err = edalloc(&e.error, 1);
   if (err == cudaSuccess) err = edalloc(&e.sums, (size_t)3 * nrep);
-  if (err == cudaSuccess) err = edalloc(&x->cell_rep, cells);
   if (err == cudaSuccess) err = edalloc(&x->d_flags, 4);
   if (err == cudaSuccess) err = cudaMemsetAsync(x->d_flags, 0, 4 * sizeof(int), x->stream);
   if (err == cudaSuccess) err = edalloc(&x->d_count, 1);
+  if (err == cudaSuccess) err = edalloc(&x->d_lists, 2 * (3 * (size_t)nrep + 5));
+  if (err == cudaSuccess) {
+    // each list: rep[nrep], atom_prefix[nrep + 1], cell_prefix[nrep + 1], count[3]
+    WorkList *w[2] = {&e.wd, &e.wb};
+    int *p = x->d_lists;
+    for (WorkList *l : w) {
+      l->rep = p;
+      l->atom_prefix = p + nrep;
+      l->cell_prefix = p + 2 * nrep + 1;
+      l->count = p + 3 * nrep + 2;
+      p += 3 * nrep + 5;
+    }
+    err = cudaMemsetAsync(x->d_lists, 0, sizeof(int) * 2 * (3 * (size_t)nrep + 5), x->stream);
+  }
+  if (err == cudaSuccess) {
+    int nsm = 0;
+    err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, prm->device);
+    x->work_blocks = std::max(1, nsm) * 8;
+  }
   if (err == cudaSuccess) {
     std::vector<int> rep_of(n, 0);
     for (int r = 0; r < nrep; r++)
       for (int k = 0; k < x->reps[r].n; k++) rep_of[x->reps[r].atom_off + k] = r;
     err = cudaMemcpy(drep, x->reps.data(), sizeof(Rep) * nrep, cudaMemcpyHostToDevice);
     if (err == cudaSuccess) err = cudaMemcpy(drep_of, rep_of.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
-    if (err == cudaSuccess && cells > 0)
-      err = cudaMemcpy(x->cell_rep, cell_rep.data(), sizeof(int) * cells, cudaMemcpyHostToDevice);
     // the slot after every replica's last cell is the next replica's first atom
     std::vector<int> starts(cells + 1, 0);
     for (int r = 0; r < nrep; r++) starts[x->reps[r].cell_off] = x->reps[r].atom_off;
@@ -1337,11 +1481,12 @@ mdg_status mdg_ensemble_kernel_time(mdg_ensemble *x, double *force_ms, int64_t *
   if (force_launches) *force_launches = x->force_launches;
   if (kernel_launches) {
     // the host counts the unconditional kernels; the branches taken (in
-    // graphs or eager steps) are counted on the device (3 and 9 kernels)
+    // graphs or eager steps) are counted on the device
     int branch[2] = {0, 0};
     ECUDA(cudaMemcpyAsync(branch, x->d_flags + 2, sizeof branch, cudaMemcpyDeviceToHost, x->stream));
     ECUDA(cudaStreamSynchronize(x->stream));
-    *kernel_launches = x->kernel_launches + 3ll * branch[0] + 9ll * branch[1];
+    *kernel_launches = x->kernel_launches + (long long)kEDispKernels * branch[0] +
+                       (long long)kEBuildKernels * branch[1];
   }
   return MDG_OK;
 }
