@@ -856,13 +856,11 @@ __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
           const int beg = a.cell_start[nc], end = a.cell_start[nc + 1];
           const int need = needed_strips(sx, sy, sz);
           const int shift = (STAGE && npl > 0) ? stage_shift(plan, npl, nc) : 0;
-          for (int j = beg; j < end; j++) {
-            const float4 lj = a.qloc[j];
-            const float ex = lj.x + bx, ey = lj.y + by, ez = lj.z + bz;
-            const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-            if (r2 > hi || j == i) continue;
-            if (need && (a.mult[j] & need) != need) continue;
-            if (r2 >= lo && !within_search_exact(a.q[i], a.q[j], sx, sy, sz, b.sl2)) continue;
+          // one candidate, in row order (FP32 prefilter, ghost rule, exact band)
+          auto accept = [&](int j, float r2) {
+            if (r2 > hi || j == i) return;
+            if (need && (a.mult[j] & need) != need) return;
+            if (r2 >= lo && !within_search_exact(a.q[i], a.q[j], sx, sy, sz, b.sl2)) return;
             if (cnt < maxnb) {
               a.nbr[(size_t)cnt * stride + i] = j;
               if (STAGE && npl > 0) {
@@ -875,7 +873,21 @@ __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
               }
             }
             cnt++;
+          };
+          auto dist2f = [&](const float4 &lj) {
+            const float ex = lj.x + bx, ey = lj.y + by, ez = lj.z + bz;
+            return fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+          };
+          // two candidates per iteration: both loads issue before either
+          // test (the loop is bound by their latency)
+          int j = beg;
+          for (; j + 1 < end; j += 2) {
+            const float4 l0 = a.qloc[j], l1 = a.qloc[j + 1];
+            const float r0 = dist2f(l0), r1 = dist2f(l1);
+            accept(j, r0);
+            accept(j + 1, r1);
           }
+          if (j < end) accept(j, dist2f(a.qloc[j]));
         }
       }
     }
