@@ -562,16 +562,27 @@ __device__ __forceinline__ int ens_build_row(const Ens &e, int i) {
           const int nc = rep.cell_off + (z * rep.ms[1] + y) * rep.ms[0] + x;
           const int beg = e.cell_start[nc], end = e.cell_start[nc + 1];
           const int need = needed_strips(sx, sy, sz);
-          for (int j = beg; j < end; j++) {
-            const float4 lj = e.qloc[j];
-            const float ex = lj.x + bx, ey = lj.y + by, ez = lj.z + bz;
-            const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-            if (r2 > hi || j == i) continue;
-            if (need && (e.mult[j] & need) != need) continue;
-            if (r2 >= lo && !within_search_exact(e.q[i], e.q[j], sx, sy, sz, e.sl2)) continue;
+          // one candidate, in row order (as the single-system build)
+          auto accept = [&](int j, float r2) {
+            if (r2 > hi || j == i) return;
+            if (need && (e.mult[j] & need) != need) return;
+            if (r2 >= lo && !within_search_exact(e.q[i], e.q[j], sx, sy, sz, e.sl2)) return;
             if (cnt < maxnb) e.nbr[(size_t)cnt * stride + i] = j;
             cnt++;
+          };
+          auto dist2f = [&](const float4 &lj) {
+            const float ex = lj.x + bx, ey = lj.y + by, ez = lj.z + bz;
+            return fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+          };
+          // two candidates per iteration, both loads issued first
+          int j = beg;
+          for (; j + 1 < end; j += 2) {
+            const float4 l0 = e.qloc[j], l1 = e.qloc[j + 1];
+            const float r0 = dist2f(l0), r1 = dist2f(l1);
+            accept(j, r0);
+            accept(j + 1, r1);
           }
+          if (j < end) accept(j, dist2f(e.qloc[j]));
         }
       }
     }
