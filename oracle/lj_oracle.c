@@ -1,6 +1,6 @@
 /*
  * CPU restatement of the MDACP single-domain LJ timestep.  TEST
- * INFRASTRUCTURE ONLY (the checker); see lj_oracle.h for the file:line map.
+ * INFRASTRUCTURE ONLY (the oracle); see lj_oracle.h for the file:line map.
  * Compile with -ffp-contract=off: every floating-point expression below keeps
  * the reference's evaluation order and must not be fused.
  */

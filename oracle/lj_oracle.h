@@ -1,7 +1,7 @@
 /*
  * CPU restatement of the MDACP Lennard-Jones timestep (kohnakagawa/mdacp) for
  * ONE domain covering the whole periodic box.  TEST INFRASTRUCTURE ONLY: it is
- * the checker that tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
+ * the oracle that tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
  * leg compare the CUDA product against; nothing in the product links it.
  *
  * It follows the reference step by step, in the same order and with the same

@@ -1,6 +1,6 @@
 """Python access to the CPU oracle.  TEST INFRASTRUCTURE ONLY.
 
-Two checkers live here:
+Two oracles live here:
 
 * ``Oracle``: ctypes binding of ``liblj_oracle.so``, the C restatement of the
   reference's single-domain timestep (lj_oracle.c; file:line map in lj_oracle.h).

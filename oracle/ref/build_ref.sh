@@ -6,7 +6,7 @@
 # compile-time CUTOFF_LENGTH (include/mdconfig.h:31) set to the cut-off the
 # workload needs, which is how the reference is configured for another rc.
 #
-# Outputs (git-ignored, they travel with the tree to the GPU box):
+# Outputs (git-ignored; the tests and bench.py run the built binaries):
 #   oracle/_ref/mdacp_rc25_plain  oracle/_ref/mdacp_rc30_plain   (-ffp-contract=off, SSE2: bit-exact oracle)
 #   oracle/_ref/mdacp_rc25_avx2   oracle/_ref/mdacp_rc30_avx2    (-DAVX2 -mavx2 -mfma: timed CPU baseline)
 #

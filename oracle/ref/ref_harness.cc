@@ -1,7 +1,7 @@
 // Test-only MDACP "Project" that drives the reference's own hot path on an
 // injected state.  It is compiled together with the unmodified reference
 // sources (src/*.cc of kohnakagawa/mdacp) into oracle/_ref/ and is used only
-// as a checker (golden fixtures) and as the timed CPU baseline.  It is never
+// to make golden fixtures and as the timed CPU baseline.  It is never
 // linked into the product.
 //
 // Registration follows the reference's own plugin mechanism: a static
