@@ -249,11 +249,11 @@ mdg_status mdg_ensemble_set_graph_mode(mdg_ensemble *e, int use_graphs);
    mdg_kernel_time for one handle: CUDA events around every force launch
    (one launch covers all replicas) while timing is on. */
 mdg_status mdg_ensemble_set_kernel_timing(mdg_ensemble *e, int on);
+mdg_status mdg_ensemble_kernel_time(mdg_ensemble *e, double *force_ms, int64_t *force_launches,
+                                    int64_t *kernel_launches);
 /* Over all replicas: neighbour-list entries of the current lists and the
    unordered pairs closer than the cut-off at the current positions. */
 mdg_status mdg_ensemble_list_stats(mdg_ensemble *e, int64_t *list_entries, int64_t *pairs_within_cutoff);
-mdg_status mdg_ensemble_kernel_time(mdg_ensemble *e, double *force_ms, int64_t *force_launches,
-                                    int64_t *kernel_launches);
 void *mdg_ensemble_stream(mdg_ensemble *e);
 
 /* ---------------------------------------------------------- box and grid analysis
