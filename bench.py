@@ -465,7 +465,11 @@ def main_mdg(args, ws, rank, local, state, config):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": dict(config, precision="fp32_mixed: FP32 pair forces on fixed-point minimum-image "
                                          "displacements, FP64 per-atom sums, integration and reductions",
-                       rebuilds=rebuilds, mean_row=entries / n),
+                       rebuilds=rebuilds, mean_row=entries / n,
+                       tuned={"threads_per_atom": r32["info1"]["threads_per_atom"],
+                              "build_block": r32["info1"]["build_block"],
+                              "fp64_build_block": r64["info1"]["build_block"],
+                              "how": "timed once per device and problem shape at the first step"}),
         "fp64": {"value": r64["value"], "ms_per_md_step": r64["ms"] / (args.steps * args.md_steps_per_step),
                  "speedup_fp32_over_fp64": r32["value"] / r64["value"]},
         "ms_per_md_step": r32["ms"] / (args.steps * args.md_steps_per_step),
@@ -568,10 +572,37 @@ def main_adjoint(args, ws, rank, local):
     return 0
 
 
+def replica_share(reps, ws, rank, search_length=2.8):
+    """The replicas of one 256-replica ensemble this rank advances: the
+    balanced partition of mdg_partition_replicas (load = atoms x (41 +
+    neighbours within the search length)); returns (indices, loads per rank)."""
+    import mdacp_b200 as M
+
+    owner, load = M.partition_replicas([(r.n, r.L) for r in reps], ws, search_length)
+    return [k for k in range(len(reps)) if owner[k] == rank], load
+
+
+def gather_replica_metrics(dist, nrep, mine, values, device=None):
+    """Per-replica metrics of every rank's share, summed into full arrays
+    (a replica belongs to exactly one rank; the others contribute zeros):
+    values is a (len(mine), m) array; returns (nrep, m) on every rank."""
+    import torch
+
+    full = np.zeros((nrep, values.shape[1]), dtype=np.float64)
+    full[mine] = values
+    if dist is None:
+        return full
+    t = torch.tensor(full, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.cpu().numpy()
+
+
 def main_ensemble(args, ws, rank, local):
     """256 independent replicas (N 500-20000, rho 0.3-0.9, T 0.7-1.5, jittered
     FCC) in one mdg_ensemble, FP32-mixed, against looping the single-system
-    handle over the same replicas."""
+    handle over the same replicas.  Under torchrun the 256 replicas are
+    partitioned over the ranks (replica_share) and every rank advances its
+    share; per-replica rebuild counts and energies are gathered to rank 0."""
     import torch
 
     import mdacp_b200 as M
@@ -580,7 +611,10 @@ def main_ensemble(args, ws, rank, local):
     dist = init_dist(ws, "nccl")
     device = f"cuda:{local}"
     torch.cuda.set_device(local)
-    reps = W.config_c4(seed=404 + rank)
+    all_reps = W.config_c4(seed=404)
+    mine, loads = replica_share(all_reps, ws, rank)
+    reps = [all_reps[k] for k in mine]
+    ntot_all = sum(r.n for r in all_reps)
     ntot = sum(r.n for r in reps)
     mdn = args.md_steps_per_step
     ens = M.Ensemble([(r.q, r.v, r.L) for r in reps], cutoff=2.5, time_step=0.005, precision=M.FP32_MIXED,
@@ -604,11 +638,21 @@ def main_ensemble(args, ws, rank, local):
     e1.synchronize()
     clocks = sampler.stop()
     ms = max_over_ranks(dist, e0.elapsed_time(e1), device)
-    value = ws * ntot * args.steps * mdn / (ms * 1e-3)
+    value = ntot_all * args.steps * mdn / (ms * 1e-3)
     fms, flaunch, launches = ens.kernel_time()
     ens.set_kernel_timing(False)
     entries, pairs = ens.list_stats()
     rb, _ = ens.rebuilds()
+    ke, pe, _ = ens.observe()
+    per_rep = gather_replica_metrics(dist, len(all_reps), mine,
+                                     np.stack([np.asarray(rb, dtype=np.float64), ke, pe], axis=1), device)
+    rb_all = per_rep[:, 0]
+    if dist is not None:
+        t = torch.tensor([float(pairs), float(entries)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        pairs, entries_all = int(t[0].item()), int(t[1].item())
+    else:
+        entries_all = entries
     ens.close()
     # roofline of the ensemble's FP32 force pass (kick + second half drift,
     # all replicas in one launch): own fixed-point copy, row length, list,
@@ -622,7 +666,7 @@ def main_ensemble(args, ws, rank, local):
     # single-system cell grid and are left out of the loop)
     loop_steps = max(20, mdn // 5)
     sl = 2.5 + 0.3
-    looped = [r for r in reps if min(int(x / sl) for x in r.L) >= 3]
+    looped = [r for r in reps if min(int(x / sl) for x in r.L) >= 3] if ws == 1 else []
     loop_n = sum(r.n for r in looped)
     systems = []
     for r in looped:
@@ -636,24 +680,32 @@ def main_ensemble(args, ws, rank, local):
         sy.calculate(loop_steps)
     torch.cuda.synchronize()
     loop_s = time.perf_counter() - t0
-    loop_value = loop_n * loop_steps / loop_s
+    loop_value = loop_n * loop_steps / loop_s if looped else None
     for sy in systems:
         sy.close()
     line = {
         "metric": "LJ atom-steps/s, 256-replica ensemble (N 500-20000)", "value": value, "unit": UNIT,
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"256 replicas, {ntot} atoms in total, N 500-20000, rho 0.3-0.9, T 0.7-1.5, "
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"256 replicas, {ntot_all} atoms in total, N 500-20000, rho 0.3-0.9, T 0.7-1.5, "
                                "jittered FCC, rc 2.5, search length 2.8, dt 0.005, NVE, FP32-mixed",
-                   "md_steps_per_step": mdn, "replicas": len(reps), "atoms": ntot,
-                   "rebuilds_per_replica_mean": float(np.mean(rb)),
+                   "md_steps_per_step": mdn, "replicas": len(all_reps), "atoms": ntot_all,
+                   "rebuilds_per_replica_mean": float(np.mean(rb_all)),
+                   "rebuilds_per_replica_max": float(np.max(rb_all)),
+                   "energy_per_atom_mean": float(np.mean((per_rep[:, 1] + per_rep[:, 2]) /
+                                                         np.array([r.n for r in all_reps]))),
+                   "partition": {"ranks": ws, "replicas_rank0": len(reps), "atoms_rank0": ntot,
+                                 "load_imbalance": float(loads.max() / loads.mean() - 1.0),
+                                 "rule": "largest load first to the least loaded rank; load = atoms x "
+                                         "(41 + neighbours within the search length)"},
+                   "parallelism": "replica partition" if ws > 1 else "single",
                    "l2": "inputs larger than L2 (state 160 MB + pairlists)"},
         "looped_single_system": {"value": loop_value, "unit": UNIT, "md_steps": loop_steps,
                                  "replicas": len(looped), "atoms": loop_n,
                                  "note": "one handle per replica with >= 3 cells per axis, calculate() in "
                                          "turn, host wall clock"},
-        "speedup_vs_looped": value / loop_value,
-        "pair_interactions_per_s": {"fp32": ws * pairs * args.steps * mdn / (ms * 1e-3),
+        "speedup_vs_looped": value / loop_value if loop_value else None,
+        "pair_interactions_per_s": {"fp32": pairs * args.steps * mdn / (ms * 1e-3),
                                     "pairs_within_cutoff_per_step": pairs},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": None, "kernel": "ke_force_fp32 (kick + second half drift, all replicas)",

@@ -73,7 +73,25 @@ typedef struct {
   int stage_atoms;          /* FP32-mixed: partner positions staged in shared memory per
                                128-atom block, at most this many atoms; 0 (default) = off,
                                partners gathered from global memory; -1 = 2304 atoms */
+  int threads_per_atom;     /* FP32-mixed force pass: lanes per atom, 1, 2 or 4; every
+                               choice gives bit-identical forces (fixed summation tree).
+                               0 (default) = chosen by timing the three once per device
+                               and problem shape, at the first step */
+  int build_block;          /* list build: threads per block, 64, 128 or 256; 0
+                               (default) = chosen by timing, as threads_per_atom */
+  int build_threads_per_atom; /* list build: lanes per atom, 1, 2 or 4 (the rows are the
+                               same for every choice); 0 (default) = chosen by timing
+                               together with build_block */
+  int step_mode;            /* how mdg_calculate runs FP32-mixed NVE steps:
+                               MDG_STEPS_AUTO (default): persistent when every atom's lanes
+                               fit in one wave of co-resident blocks, else graphs;
+                               MDG_STEPS_GRAPHS: CUDA graphs with conditional rebuild nodes;
+                               MDG_STEPS_PERSISTENT: one cooperative launch runs the steps
+                               back to back until one needs the displacement check or a
+                               rebuild, which then runs as an ordinary step.  Same results. */
 } mdg_params;
+
+enum { MDG_STEPS_AUTO = 0, MDG_STEPS_GRAPHS = 1, MDG_STEPS_PERSISTENT = 2 };
 
 /* Fills p with the reference defaults (SimulationInfo ctor, src/simulationinfo.cc:5-51). */
 void mdg_default_params(mdg_params *p);
@@ -184,6 +202,10 @@ typedef struct {
   int64_t displacement_checks;
   double simulation_time;
   double buffer_left;     /* skin budget (PairList::buffer_length) */
+  int threads_per_atom;   /* lanes per atom of the FP32-mixed force pass (0: not chosen yet) */
+  int build_block;        /* threads per block of the list build (0: not chosen yet) */
+  int build_threads_per_atom; /* lanes per atom of the list build (0: not chosen yet) */
+  int64_t persistent_steps;   /* steps taken by the persistent pass (step_mode) */
 } mdg_info;
 mdg_status mdg_get_info(mdg_handle *h, mdg_info *info);
 
@@ -211,9 +233,15 @@ mdg_status mdg_kernel_time(mdg_handle *h, double *force_ms, int64_t *force_launc
    are host values.  Work is queued on `stream` (cudaStream_t, NULL = legacy
    default stream); out is ready when the stream is.  Scratch is a static
    device array of 196,608 bytes held by every GPU that loads the library, so
-   n is limited to 2,097,152 (MDG_ERR_CAPACITY above).  The first call on a
-   device sets up the array's address: make it before any stream capture.
-   Calls that overlap on the GPU race on the shared scratch. */
+   n is limited to 2,097,152 (MDG_ERR_CAPACITY above).  A call outside a
+   stream capture looks the array's address up with its device current; a
+   call during a capture uses the address found by the last uncaptured call
+   on that device (MDG_ERR_STATE if there was none), so make one call per
+   device before capturing.  Calls that overlap on the GPU race on the
+   shared scratch.  A partner index outside [0, n) is never read: the pair
+   is skipped and the returned PE is NaN.  A CUDA error already pending from
+   the caller's earlier work is left pending and reported as MDG_ERR_CUDA
+   with nothing launched. */
 mdg_status mdg_observe_static(const double *q4, const double *v4, int n, const int *row_start,
                               const int *partners, const double L[3], double cutoff, double *out,
                               void *stream);
@@ -256,6 +284,56 @@ mdg_status mdg_ensemble_kernel_time(mdg_ensemble *e, double *force_ms, int64_t *
 mdg_status mdg_ensemble_list_stats(mdg_ensemble *e, int64_t *list_entries, int64_t *pairs_within_cutoff);
 void *mdg_ensemble_stream(mdg_ensemble *e);
 
+/* Replaces, for independent replicas, the reference's assignment of work
+   to MPI ranks (ParaInfo, src/parainfo.cc:16-94, which splits one box into a
+   grid of equal domains): replica r goes to rank owner[r] so that the
+   ranks' loads are balanced, the load of a replica being its atoms times
+   (41 + the neighbours expected within search_length, 4/3 pi SL^3 N/V) --
+   the list entries a step streams per atom plus the per-atom state traffic
+   in the same 4-byte units (164 B).  Largest load first, each to the least
+   loaded rank (lowest rank on ties): deterministic.  load (nranks doubles,
+   may be NULL) returns every rank's total.  Host-only: no device needed. */
+mdg_status mdg_partition_replicas(const mdg_replica *replicas, int nrep, double search_length, int nranks,
+                                  int *owner, double *load);
+
+/* ---------------------------------------------------------- slab decomposition
+ * One periodic system split into z-slabs of whole cell layers of the
+ * single-domain cell grid (int(L/SL) cells per axis), one slab per device
+ * (devices may repeat), driven by the calling thread.  Replaces the
+ * reference's domain decomposition: migration MDManager::SendParticles
+ * (src/mdmanager.cc:317-374), ghost layers refreshed every step
+ * MDManager::SendBorderParticles (src/mdmanager.cc:419-489,
+ * src/mdunit.cc:140-208), the expiry all-reduce (src/mdmanager.cc:509-518,
+ * src/communicator.cc:24-37).  Each slab holds its own atoms plus one ghost
+ * layer of cells on each side; every step each slab pushes its two border
+ * layers' positions into its neighbours' ghost slots (peer copies); the
+ * skin decision, the displacement check and the rebuild are global, and a
+ * rebuild migrates the atoms that changed slab.  Lists, force sums and
+ * trajectories equal the single domain's.  NVE, FP64 or FP32-mixed;
+ * host-driven steps (one host synchronisation per step for the global skin
+ * decision).  Layers are split as evenly as their count allows; at least
+ * one layer per slab, at least 2 slabs. */
+typedef struct mdg_slabs mdg_slabs;
+/* params: the whole system's box, capacity (all atoms), cutoff, buffer
+   length, time step, precision, check_list_length, threads_per_atom;
+   devices: nslabs device ordinals, or NULL for params->device. */
+mdg_status mdg_slabs_create(const mdg_params *params, int nslabs, const int *devices, mdg_slabs **out);
+mdg_status mdg_slabs_destroy(mdg_slabs *x);
+/* n atoms in the reference's AoS layout (as mdg_set_state); each goes to the
+   slab of its cell layer; ids are the upload indices. */
+mdg_status mdg_slabs_set_state(mdg_slabs *x, const double *q4, const double *v4, const int *type, int n);
+/* n x 4 doubles ordered by upload index. */
+mdg_status mdg_slabs_get_state(mdg_slabs *x, double *q4, double *v4, int n);
+mdg_status mdg_slabs_calculate(mdg_slabs *x, int nsteps);
+/* System sums over all slabs, as mdg_observe (MDG_OBSERVE_CURRENT). */
+mdg_status mdg_slabs_observe(mdg_slabs *x, double *ke, double *pe, double *virial);
+/* Forces (no kick) ordered by upload index, n x 4 doubles, as mdg_forces. */
+mdg_status mdg_slabs_forces(mdg_slabs *x, double *f4, int n);
+/* Steps, rebuilds, and per slab its own atoms and ghost copies (arrays of
+   nslabs ints, may be NULL). */
+mdg_status mdg_slabs_info(mdg_slabs *x, int64_t *steps, int64_t *rebuilds, int *owned, int *ghosts);
+const char *mdg_slabs_last_error(mdg_slabs *x);
+
 /* ---------------------------------------------------------- box and grid analysis
  * MDManager::ChangeScale (src/mdmanager.cc:573-585) on the device: the list
  * is built (atoms wrapped into the box), the box and every position are
@@ -285,9 +363,13 @@ mdg_status mdg_load_checkpoint(mdg_handle *h, const char *path);
  * MDUnit::SaveAsCdview ("0 type x y z px py pz", src/mdunit.cc:67-83),
  * CONFIGURATION as Variables::SaveConfiguration ("x y z px py pz",
  * src/variables.cc:49-61).  The device-to-host copy is queued on the
- * handle's stream and a host thread writes the file, so the caller can keep
- * queuing steps; mdg_snapshot_wait joins every pending writer and reports
- * the first failure. */
+ * handle's stream into pinned buffers the handle keeps (allocated on the
+ * first call, grown with the atom count) and a host thread writes the file,
+ * so the caller can keep queuing steps.  At most one file is pending: a call
+ * first waits for the previous file and, if that write failed, returns
+ * MDG_ERR_IO with its name and starts nothing.  mdg_snapshot_wait waits for
+ * the pending file and reports its failure the same way; call it before
+ * mdg_destroy, which waits too but cannot report. */
 enum { MDG_SNAPSHOT_CDVIEW = 0, MDG_SNAPSHOT_CONFIGURATION = 1 };
 mdg_status mdg_snapshot_async(mdg_handle *h, const char *path, int format);
 mdg_status mdg_snapshot_wait(mdg_handle *h);

@@ -81,7 +81,14 @@ class Params(ctypes.Structure):
         ("device", ctypes.c_int),
         ("stream", ctypes.c_void_p),
         ("stage_atoms", ctypes.c_int),
+        ("threads_per_atom", ctypes.c_int),
+        ("build_block", ctypes.c_int),
+        ("build_threads_per_atom", ctypes.c_int),
+        ("step_mode", ctypes.c_int),
     ]
+
+
+STEPS_AUTO, STEPS_GRAPHS, STEPS_PERSISTENT = 0, 1, 2
 
 
 class Info(ctypes.Structure):
@@ -98,6 +105,10 @@ class Info(ctypes.Structure):
         ("displacement_checks", ctypes.c_int64),
         ("simulation_time", ctypes.c_double),
         ("buffer_left", ctypes.c_double),
+        ("threads_per_atom", ctypes.c_int),
+        ("build_block", ctypes.c_int),
+        ("build_threads_per_atom", ctypes.c_int),
+        ("persistent_steps", ctypes.c_int64),
     ]
 
     def as_dict(self):
@@ -206,6 +217,17 @@ SIGNATURES = {
     "mdg_ensemble_rebuilds": (ctypes.c_int, [_H, _I64P, _I64P]),
     "mdg_ensemble_set_graph_mode": (ctypes.c_int, [_H, ctypes.c_int]),
     "mdg_ensemble_stream": (ctypes.c_void_p, [_H]),
+    "mdg_slabs_create": (ctypes.c_int, [ctypes.POINTER(Params), ctypes.c_int, _IP, ctypes.POINTER(_H)]),
+    "mdg_slabs_destroy": (ctypes.c_int, [_H]),
+    "mdg_slabs_set_state": (ctypes.c_int, [_H, _DP, _DP, _IP, ctypes.c_int]),
+    "mdg_slabs_get_state": (ctypes.c_int, [_H, _DP, _DP, ctypes.c_int]),
+    "mdg_slabs_calculate": (ctypes.c_int, [_H, ctypes.c_int]),
+    "mdg_slabs_observe": (ctypes.c_int, [_H, _DP, _DP, _DP]),
+    "mdg_slabs_forces": (ctypes.c_int, [_H, _DP, ctypes.c_int]),
+    "mdg_slabs_info": (ctypes.c_int, [_H, _I64P, _I64P, _IP, _IP]),
+    "mdg_slabs_last_error": (ctypes.c_char_p, [_H]),
+    "mdg_partition_replicas": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _IP,
+                                              _DP]),
     "mdg_ensemble_set_kernel_timing": (ctypes.c_int, [_H, ctypes.c_int]),
     "mdg_ensemble_kernel_time": (ctypes.c_int, [_H, _DP, _I64P, _I64P]),
     "mdg_ensemble_list_stats": (ctypes.c_int, [_H, _I64P, _I64P]),
@@ -256,7 +278,8 @@ class System:
     def __init__(self, L, cutoff=2.5, time_step=0.005, capacity=None, precision=FP64,
                  thermostat=NVE, aimed_temperature=1.0, heatbath_tau=0.1, heatbath_gamma=0.1,
                  seed=0, buffer_length=0.3, check_list_length=500, max_neighbors=0, device=0,
-                 stream=None, n_hint=None, stage_atoms=0):
+                 stream=None, n_hint=None, stage_atoms=0, threads_per_atom=0, build_block=0,
+                 build_threads_per_atom=0, step_mode=0):
         self.lib = load_library()
         p = Params()
         self.lib.mdg_default_params(ctypes.byref(p))
@@ -276,6 +299,10 @@ class System:
         p.device = int(device)
         p.stream = stream
         p.stage_atoms = int(stage_atoms)
+        p.threads_per_atom = int(threads_per_atom)
+        p.build_block = int(build_block)
+        p.build_threads_per_atom = int(build_threads_per_atom)
+        p.step_mode = int(step_mode)
         self.params = p
         h = _H()
         st = self.lib.mdg_create(ctypes.byref(p), ctypes.byref(h))
@@ -506,15 +533,117 @@ class System:
         return ms.value, fl.value, kl.value
 
 
+class Slabs:
+    """One periodic system split into z-slabs of cell layers, one slab per
+    device (mdg_slabs_*); ``devices`` lists a device per slab (default: all
+    on ``device``)."""
+
+    def __init__(self, L, nslabs, cutoff=2.5, time_step=0.005, capacity=None, precision=FP64, buffer_length=0.3,
+                 check_list_length=500, device=0, devices=None, threads_per_atom=0):
+        self.lib = load_library()
+        p = Params()
+        self.lib.mdg_default_params(ctypes.byref(p))
+        p.capacity = int(capacity or 1)
+        p.L[:] = [float(x) for x in L]
+        p.cutoff = float(cutoff)
+        p.buffer_length = float(buffer_length)
+        p.time_step = float(time_step)
+        p.precision = int(precision)
+        p.check_list_length = int(check_list_length)
+        p.device = int(device)
+        p.threads_per_atom = int(threads_per_atom)
+        self.nslabs = int(nslabs)
+        devs = None
+        if devices is not None:
+            devs = np.ascontiguousarray(devices, dtype=np.int32)
+        h = _H()
+        st = self.lib.mdg_slabs_create(ctypes.byref(p), self.nslabs, _i(devs) if devs is not None else None,
+                                       ctypes.byref(h))
+        if st != 0:
+            raise MdgError(st, self.lib.mdg_status_string(st).decode())
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mdg_slabs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != 0:
+            raise MdgError(st, (self.lib.mdg_slabs_last_error(self.h) or b"").decode())
+
+    def set_state(self, q, v, type_=None):
+        q4 = _pad4(np.asarray(q, dtype=np.float64))
+        v4 = _pad4(np.asarray(v, dtype=np.float64))
+        t = np.ascontiguousarray(type_, dtype=np.int32) if type_ is not None else None
+        self._check(self.lib.mdg_slabs_set_state(self.h, _d(q4), _d(v4), _i(t) if t is not None else None,
+                                                 q4.shape[0]))
+        self.n = q4.shape[0]
+
+    def state_by_id(self):
+        q4 = np.empty((self.n, 4))
+        v4 = np.empty((self.n, 4))
+        self._check(self.lib.mdg_slabs_get_state(self.h, _d(q4), _d(v4), self.n))
+        return q4[:, :3].copy(), v4[:, :3].copy()
+
+    def calculate(self, nsteps=1):
+        self._check(self.lib.mdg_slabs_calculate(self.h, int(nsteps)))
+
+    def observe(self):
+        ke, pe, vir = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mdg_slabs_observe(self.h, ctypes.byref(ke), ctypes.byref(pe), ctypes.byref(vir)))
+        return ke.value, pe.value, vir.value
+
+    def forces_by_id(self):
+        f4 = np.empty((self.n, 4))
+        self._check(self.lib.mdg_slabs_forces(self.h, _d(f4), self.n))
+        return f4[:, :3].copy()
+
+    def info(self):
+        steps, rebuilds = ctypes.c_int64(), ctypes.c_int64()
+        owned = np.zeros(self.nslabs, dtype=np.int32)
+        ghosts = np.zeros(self.nslabs, dtype=np.int32)
+        self._check(self.lib.mdg_slabs_info(self.h, ctypes.byref(steps), ctypes.byref(rebuilds), _i(owned),
+                                            _i(ghosts)))
+        return {"steps": steps.value, "rebuilds": rebuilds.value, "owned": owned.tolist(), "ghosts": ghosts.tolist()}
+
+
+def partition_replicas(boxes, nranks, search_length=2.8):
+    """Balanced assignment of independent replicas to ranks
+    (mdg_partition_replicas): ``boxes`` is a list of (n_atoms, L); returns
+    (owner per replica, load per rank)."""
+    lib = load_library()
+    nrep = len(boxes)
+    reps = (Replica * max(nrep, 1))()
+    for k, (n, L) in enumerate(boxes):
+        reps[k].n = int(n)
+        reps[k].L[:] = [float(x) for x in L]
+    owner = np.zeros(max(nrep, 1), dtype=np.int32)
+    load = np.zeros(nranks, dtype=np.float64)
+    st = lib.mdg_partition_replicas(ctypes.cast(reps, ctypes.c_void_p), nrep, float(search_length), int(nranks),
+                                    _i(owner), _d(load))
+    if st != 0:
+        raise MdgError(st, "mdg_partition_replicas")
+    return owner[:nrep], load
+
+
 class Ensemble:
     """Independent periodic replicas advanced together (mdg_ensemble_*).
     ``states`` is a list of (q, v, L) per replica."""
 
     def __init__(self, states, cutoff=2.5, time_step=0.005, precision=FP64, buffer_length=0.3,
-                 check_list_length=500, device=0):
+                 check_list_length=500, device=0, threads_per_atom=0):
         self.lib = load_library()
         p = Params()
         self.lib.mdg_default_params(ctypes.byref(p))
+        p.threads_per_atom = int(threads_per_atom)
         p.cutoff = float(cutoff)
         p.time_step = float(time_step)
         p.precision = int(precision)

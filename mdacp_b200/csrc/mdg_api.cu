@@ -9,7 +9,9 @@
 #include <cstring>
 #include <atomic>
 #include <fstream>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <thread>
 #include <vector>
@@ -42,6 +44,9 @@ bool box_geometry(mdg::Box &b, const double L[3], double SL) {
     const int ms = (int)(L[d] / SL);
     if (ms < 3) return false;
   }
+  b.sl = SL;
+  b.sl2 = SL * SL;
+  mdg::prefilter_band(b.sl2, SL, L[0], &b.sl2_lo, &b.sl2_hi);
   for (int d = 0; d < 3; d++) {
     b.L[d] = L[d];
     b.hL[d] = 0.5 * L[d];
@@ -51,8 +56,17 @@ bool box_geometry(mdg::Box &b, const double L[3], double SL) {
     b.cs[d] = L[d] / (double)b.ms[d];
   }
   b.ncell = b.ms[0] * b.ms[1] * b.ms[2];
+  b.slab = 0;
+  b.z0 = 0;
+  b.nzl = b.ms[2];
   return true;
 }
+
+// The list build packs cell coordinates into one int (pack_cell).
+bool cells_packable(const mdg::Box &b) { return b.ms[0] < 2048 && b.ms[1] < 2048 && b.ms[2] < 1024; }
+
+// Entries of the list build's trim table: one block of 8 ms_x + 1 per x-row.
+size_t trim_table_size(const mdg::Box &b) { return (size_t)b.ms[1] * b.ms[2] * (b.ms[0] * kXSub + 1); }
 
 }  // namespace
 
@@ -87,10 +101,20 @@ struct mdg_handle {
   // every atom's position after the coming step's first half drift; -1: none
   int fix_buf = -1;
   int cell_cap = 0;                   // cells the cell tables hold
+  int tpa = 0;                        // lanes per atom of the FP32 force pass (0: to be tuned)
+  int build_block = 0;                // threads per block of the list build (0: to be tuned)
+  int build_tpa = 0;                  // lanes per atom of the list build (0: to be tuned)
+  GridBarrier *d_bar = nullptr;       // persistent pass: grid barrier
+  int *d_pout = nullptr;              // persistent pass: steps taken, buffer parity, decision
+  int64_t persistent_steps = 0;
   External ext{};                     // executor applied after every step (kind 0: none)
-  std::vector<std::thread> writers;   // pending snapshot writers
-  std::mutex writer_mutex;
-  std::string writer_error;           // first failure of a writer
+  // snapshots: one set of pinned buffers per handle, at most one pending writer
+  std::thread writer;
+  std::string writer_error;           // failure of the last writer (read after joining it)
+  double4 *snap_q = nullptr, *snap_v = nullptr;
+  int *snap_t = nullptr;
+  int snap_cap = 0;
+  cudaEvent_t snap_done = nullptr;
   std::string err;
 };
 
@@ -115,7 +139,7 @@ cudaError_t dalloc(T **p, size_t count) {
 }
 
 void free_arrays(Arrays &a) {
-  void *ptrs[] = {a.q, a.v, a.q_old, a.qfix, a.qfix2, a.qloc, a.ids, a.type, a.cell, a.nbr, a.nnbr, a.cell_count,
+  void *ptrs[] = {a.q, a.v, a.q_old, a.qfix, a.qfix2, a.qloc, a.cxyz, a.xsub, a.ids, a.type, a.cell, a.nbr, a.nnbr, a.cell_count,
                   a.cell_start, a.slot, a.perm, a.perm2, a.q_tmp, a.v_tmp, a.ids_tmp, a.type_tmp,
                   a.cell_tmp, a.mult, a.cand, a.partials, a.st, a.stage_rng, a.stage_n, a.nbr16};
   for (void *p : ptrs)
@@ -221,6 +245,23 @@ double step_lag(const mdg_handle *h) {
 // Kernels of one rebuild (launch_build).
 int build_kernels(const mdg_handle *h) { return h->a.stage_cap > 0 ? 11 : 10; }
 
+// The list build alone (the rows of the atoms' current cell order), with
+// `block` threads per block and `lanes` threads per atom.
+template <int BLOCK>
+void launch_list_build_block(mdg_handle *h, cudaStream_t s, int lanes) {
+  const int n = h->n;
+  const int nb = (int)std::max<long long>(1, ((long long)n * lanes + BLOCK - 1) / BLOCK);
+  if (lanes == 4) k_build<BLOCK, false, false, 4><<<nb, BLOCK, 0, s>>>(h->a, h->box, n);
+  else if (lanes == 2) k_build<BLOCK, false, false, 2><<<nb, BLOCK, 0, s>>>(h->a, h->box, n);
+  else k_build<BLOCK, false, false, 1><<<nb, BLOCK, 0, s>>>(h->a, h->box, n);
+}
+
+void launch_list_build(mdg_handle *h, cudaStream_t s, int block, int lanes) {
+  if (block == 64) launch_list_build_block<64>(h, s, lanes);
+  else if (block == 256) launch_list_build_block<256>(h, s, lanes);
+  else launch_list_build_block<128>(h, s, lanes);
+}
+
 void launch_build(mdg_handle *h, cudaStream_t s, int4 *pack = nullptr) {
   const int n = h->n;
   Arrays &a = h->a;
@@ -232,7 +273,7 @@ void launch_build(mdg_handle *h, cudaStream_t s, int4 *pack = nullptr) {
   k_scan_tile_sums<kScanBlock><<<1, kScanBlock, 0, s>>>(a, h->ncell, h->d_tiles, ntiles);
   k_scan_add<kScanBlock><<<ntiles, kScanBlock, 0, s>>>(a, h->ncell, h->d_tiles);
   k_scatter<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, n);
-  k_sort_cells<<<blocks_for(h->ncell * 32, kBlock), kBlock, 0, s>>>(a, h->ncell);
+  k_sort_cells<<<blocks_for(h->ncell * 32, kBlock), kBlock, 0, s>>>(a, h->box, h->ncell);
   k_permute<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, h->box, n, pack);
   cudaMemcpyAsync(a.q, a.q_tmp, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
   cudaMemcpyAsync(a.v, a.v_tmp, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
@@ -243,7 +284,7 @@ void launch_build(mdg_handle *h, cudaStream_t s, int4 *pack = nullptr) {
     k_stage_plan<kBlock><<<blocks_for(blocks_for(n, kStageBlock), kBlock), kBlock, 0, s>>>(a, h->box, n);
     k_build<kForceBlock, true><<<blocks_for(n, kForceBlock), kForceBlock, 0, s>>>(a, h->box, n);
   } else {
-    k_build<kForceBlock, false><<<blocks_for(n, kForceBlock), kForceBlock, 0, s>>>(a, h->box, n);
+    launch_list_build(h, s, h->build_block > 0 ? h->build_block : kForceBlock, h->build_tpa > 0 ? h->build_tpa : 1);
   }
   k_build_done<<<1, 32, 0, s>>>(a, h->box);
 }
@@ -290,6 +331,20 @@ cudaError_t set_stage_smem(int atoms) {
   return e;
 }
 
+// The FP32-mixed force pass with TPA lanes per atom (drift as below).
+template <int MODE, int TPA>
+void launch_fp32(mdg_handle *h, cudaStream_t s, const Thermo &th, int drift, const int4 *qf, int4 *qf_next) {
+  const int n = h->n;
+  const int nb = (int)(((long long)n * TPA + kForceBlock - 1) / kForceBlock);
+  if (nb == 0) return;
+  if (drift == 2)
+    k_force_fp32<kForceBlock, MODE, 2, TPA><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, qf_next);
+  else if (drift)
+    k_force_fp32<kForceBlock, MODE, 1, TPA><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, nullptr);
+  else
+    k_force_fp32<kForceBlock, MODE, 0, TPA><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, nullptr);
+}
+
 // drift: 1 also applies the second half drift in the same pass, 2 the whole
 // fused NVE step reading qf and packing into qf_next (FP32-mixed only);
 // returns false when the caller still has to launch the second drift.
@@ -310,12 +365,10 @@ bool launch_force_mode(mdg_handle *h, cudaStream_t s, const Thermo &th, int drif
     return drift != 0;
   }
   if (h->prm.precision == MDG_FP32_MIXED) {
-    if (drift == 2)
-      k_force_fp32<kForceBlock, MODE, 2><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, qf_next);
-    else if (drift)
-      k_force_fp32<kForceBlock, MODE, 1><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, nullptr);
-    else
-      k_force_fp32<kForceBlock, MODE, 0><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, nullptr);
+    const int tpa = h->tpa > 0 ? h->tpa : 1;
+    if (tpa == 4) launch_fp32<MODE, 4>(h, s, th, drift, qf, qf_next);
+    else if (tpa == 2) launch_fp32<MODE, 2>(h, s, th, drift, qf, qf_next);
+    else launch_fp32<MODE, 1>(h, s, th, drift, qf, qf_next);
     return drift != 0;
   }
   k_force_fp64<kForceBlock, MODE><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th);
@@ -557,6 +610,171 @@ mdg_status ensure_list(mdg_handle *h) {
   return MDG_OK;
 }
 
+// ------------------------------------------------------------ autotuner
+// The lanes per atom of the FP32-mixed force pass (1, 2, 4) and the atoms
+// per block of the list build (64, 128, 256), chosen by timing each
+// candidate a few times on the handle's own state once its list is built,
+// and remembered per device and problem shape (atoms, cells, precision)
+// for the rest of the process.  The force candidates run force-only (the
+// forces go to scratch, the state is untouched); the build candidates
+// rebuild the same rows from the same cell order, and a last build with the
+// chosen block leaves the list counters as a normal build does.
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, int, int>, std::tuple<int, int, int>> g_tuned;
+
+template <typename F>
+float time_launches(cudaStream_t s, F launch, int reps) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float ms = -1.f;
+  if (cudaEventCreate(&e0) != cudaSuccess) return ms;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return ms;
+  }
+  launch();  // warm-up
+  cudaEventRecord(e0, s);
+  for (int k = 0; k < reps; k++) launch();
+  cudaEventRecord(e1, s);
+  if (cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms;
+}
+
+static __global__ void k_list_counters_reset(Arrays a) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    a.st->max_row = 0;
+    a.st->list_entries = 0;
+  }
+}
+
+mdg_status autotune(mdg_handle *h) {
+  const bool fp32 = h->prm.precision == MDG_FP32_MIXED;
+  if (!fp32 && h->tpa == 0) h->tpa = 1;            // the FP64 pass has one lane per atom
+  if (h->a.stage_cap > 0) {  // stage rows per 128 atoms, one lane per atom
+    if (h->build_block == 0) h->build_block = kForceBlock;
+    if (h->build_tpa == 0) h->build_tpa = 1;
+  }
+  if (h->tpa > 0 && h->build_block > 0 && h->build_tpa > 0) return MDG_OK;
+  const auto key = std::make_tuple(h->prm.device, h->n, h->ncell, h->prm.precision);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      if (h->tpa == 0) h->tpa = std::get<0>(it->second);
+      if (h->build_block == 0) h->build_block = std::get<1>(it->second);
+      if (h->build_tpa == 0) h->build_tpa = std::get<2>(it->second);
+      destroy_graph(h);
+      return MDG_OK;
+    }
+  }
+  mdg_status r = ensure_list(h);
+  if (r) return r;
+  cudaStream_t s = h->stream;
+  const int n = h->n;
+  int tpa = h->tpa, bb = h->build_block;
+  if (tpa == 0) {
+    k_pack_fix<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(h->a, h->box, n);
+    h->fix_buf = -1;  // the copy the fused step reads is repacked before the next step
+    const Thermo th = thermo_of(h);
+    float best = 0.f;
+    const int cand[3] = {1, 2, 4};
+    for (int c : cand) {
+      const float ms = time_launches(s, [&]() {
+        if (c == 4) launch_fp32<kForceOut, 4>(h, s, th, 0, h->a.qfix, nullptr);
+        else if (c == 2) launch_fp32<kForceOut, 2>(h, s, th, 0, h->a.qfix, nullptr);
+        else launch_fp32<kForceOut, 1>(h, s, th, 0, h->a.qfix, nullptr);
+      }, 5);
+      if (ms < 0.f) return fail(h, MDG_ERR_CUDA, "autotune: force timing failed");
+      if (tpa == 0 || ms < best) {
+        best = ms;
+        tpa = c;
+      }
+    }
+  }
+  int bl = h->build_tpa;
+  if (bb == 0 || bl == 0) {
+    float best = -1.f;
+    int bb_best = 0, bl_best = 0;
+    const int blocks[3] = {64, 128, 256}, lanes[3] = {1, 2, 4};
+    for (int cb : blocks) {
+      if (bb != 0 && cb != bb) continue;
+      for (int cl : lanes) {
+        if (bl != 0 && cl != bl) continue;
+        const float ms = time_launches(s, [&]() { launch_list_build(h, s, cb, cl); }, 3);
+        if (ms < 0.f) return fail(h, MDG_ERR_CUDA, "autotune: build timing failed");
+        if (best < 0.f || ms < best) {
+          best = ms;
+          bb_best = cb;
+          bl_best = cl;
+        }
+      }
+    }
+    bb = bb_best;
+    bl = bl_best;
+    k_list_counters_reset<<<1, 32, 0, s>>>(h->a);
+    launch_list_build(h, s, bb, bl);
+  }
+  CUDA_TRY(h, cudaGetLastError());
+  Status st;
+  if ((r = read_status(h, &st))) return r;
+  if (st.error) return translate_device_error(h, st);
+  h->tpa = tpa;
+  h->build_block = bb;
+  h->build_tpa = bl;
+  destroy_graph(h);
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tuned[key] = std::make_tuple(tpa, bb, bl);
+  return MDG_OK;
+}
+
+// ------------------------------------------------------- persistent steps
+// Blocks of the persistent pass for this handle: enough for every atom's
+// lanes, at most what the device keeps resident at once (a cooperative
+// launch needs all of them resident); 0 if the kernel cannot be resident.
+template <int TPA>
+int persistent_grid(mdg_handle *h) {
+  int per_sm = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nve_persistent<kForceBlock, TPA>, kForceBlock, 0) !=
+          cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->prm.device) != cudaSuccess)
+    return 0;
+  const long long need = ((long long)h->n * TPA + kForceBlock - 1) / kForceBlock;
+  return (int)std::min<long long>(need, (long long)per_sm * sms);
+}
+
+// Whether mdg_calculate runs the persistent pass: asked for, or (auto) when
+// one wave of resident blocks covers every atom's lanes.
+bool use_persistent(mdg_handle *h) {
+  if (!fused_step(h) || h->prm.step_mode == MDG_STEPS_GRAPHS) return false;
+  const int tpa = h->tpa > 0 ? h->tpa : 1;
+  const int g = tpa == 4 ? persistent_grid<4>(h) : (tpa == 2 ? persistent_grid<2>(h) : persistent_grid<1>(h));
+  if (g <= 0) return false;
+  if (h->prm.step_mode == MDG_STEPS_PERSISTENT) return true;
+  return (long long)g * kForceBlock >= (long long)h->n * tpa;
+}
+
+// Up to `steps` steps in one cooperative launch; *taken returns how many ran.
+template <int TPA>
+mdg_status launch_persistent(mdg_handle *h, int steps, int *taken) {
+  const int grid = persistent_grid<TPA>(h);
+  if (grid <= 0) return fail(h, MDG_ERR_CUDA, "persistent pass: no resident grid");
+  CUDA_TRY(h, cudaMemsetAsync(h->d_bar, 0, sizeof(GridBarrier), h->stream));
+  int n = h->n, parity = h->fix_buf > 0 ? 1 : 0;
+  int4 *q0 = h->a.qfix, *q1 = h->a.qfix2;
+  void *args[] = {&h->a, &h->box, &n, &steps, &q0, &q1, &parity, &h->d_bar, &h->d_pout};
+  CUDA_TRY(h, cudaLaunchCooperativeKernel((const void *)k_nve_persistent<kForceBlock, TPA>, dim3(grid),
+                                          dim3(kForceBlock), args, 0, h->stream));
+  int out[2] = {0, 0};
+  CUDA_TRY(h, cudaMemcpyAsync(out, h->d_pout, sizeof out, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  h->kernel_launches++;
+  h->fix_buf = out[1];
+  *taken = out[0];
+  h->persistent_steps += out[0];
+  return MDG_OK;
+}
+
 }  // namespace
 
 // ================================================================== C ABI
@@ -581,6 +799,10 @@ void mdg_default_params(mdg_params *p) {
   p->device = 0;
   p->stream = nullptr;
   p->stage_atoms = 0;
+  p->threads_per_atom = 0;        // timed at the first step
+  p->build_block = 0;             // timed at the first step
+  p->build_threads_per_atom = 0;  // timed at the first step
+  p->step_mode = MDG_STEPS_AUTO;
 }
 
 mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
@@ -589,7 +811,13 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   if (prm->capacity < 1 || prm->cutoff <= 0.0 || prm->buffer_length < 0.0 || prm->time_step <= 0.0 ||
       prm->check_list_length < 1 || (prm->precision != MDG_FP64 && prm->precision != MDG_FP32_MIXED) ||
       prm->thermostat < MDG_NVE || prm->thermostat > MDG_LANGEVIN || prm->stage_atoms < -1 ||
-      prm->stage_atoms > kStageMax)
+      prm->stage_atoms > kStageMax ||
+      (prm->threads_per_atom != 0 && prm->threads_per_atom != 1 && prm->threads_per_atom != 2 &&
+       prm->threads_per_atom != 4) ||
+      (prm->build_block != 0 && prm->build_block != 64 && prm->build_block != 128 && prm->build_block != 256) ||
+      (prm->build_threads_per_atom != 0 && prm->build_threads_per_atom != 1 && prm->build_threads_per_atom != 2 &&
+       prm->build_threads_per_atom != 4) ||
+      prm->step_mode < MDG_STEPS_AUTO || prm->step_mode > MDG_STEPS_PERSISTENT)
     return MDG_ERR_INVALID_ARGUMENT;
   for (int d = 0; d < 3; d++)
     if (!(prm->L[d] > 0.0) || !std::isfinite(prm->L[d])) return MDG_ERR_INVALID_ARGUMENT;
@@ -605,8 +833,10 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
     delete h;
     return MDG_ERR_BOX_TOO_SMALL;
   }
-  b.sl = SL;
-  b.sl2 = SL * SL;
+  if (!cells_packable(b)) {
+    delete h;
+    return MDG_ERR_INVALID_ARGUMENT;
+  }
   b.rc2 = prm->cutoff * prm->cutoff;
   b.rc = prm->cutoff;
   {  // Variables::Variables, src/variables.cc:21-27
@@ -620,12 +850,12 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   b.rc2f = (float)b.rc2;
   b.c2x8f = (float)(b.c2 * 8.0);
   b.check_list_length = prm->check_list_length;
-  // FP32 prefilter band: FP32 r^2 within 1e-4 SL^2 of SL^2 is decided in FP64
-  b.sl2_lo = (float)(b.sl2 * (1.0 - 1e-4));
-  b.sl2_hi = (float)(b.sl2 * (1.0 + 1e-4));
   h->ncell = b.ncell;
   h->cell_cap = b.ncell;
   h->cap = prm->capacity;
+  h->tpa = prm->threads_per_atom;
+  h->build_block = prm->build_block;
+  h->build_tpa = prm->build_threads_per_atom;
 
   cudaError_t e = cudaSetDevice(prm->device);
   if (e == cudaSuccess) {
@@ -648,6 +878,8 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   if (e == cudaSuccess) e = dalloc(&a.qfix, cap);
   if (e == cudaSuccess) e = dalloc(&a.qfix2, cap);
   if (e == cudaSuccess) e = dalloc(&a.qloc, cap);
+  if (e == cudaSuccess) e = dalloc(&a.cxyz, cap);
+  if (e == cudaSuccess) e = dalloc(&a.xsub, trim_table_size(b));
   if (e == cudaSuccess) e = dalloc(&a.ids, cap);
   if (e == cudaSuccess) e = dalloc(&a.type, cap);
   if (e == cudaSuccess) e = dalloc(&a.cell, cap);
@@ -669,6 +901,8 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   if (e == cudaSuccess) e = dalloc(&h->d_flags, 4);
   if (e == cudaSuccess) e = dalloc(&h->d_sums, 8);
   if (e == cudaSuccess) e = dalloc(&h->d_tiles, (size_t)blocks_for(h->ncell, kScanBlock) + 1);
+  if (e == cudaSuccess) e = dalloc(&h->d_bar, 1);
+  if (e == cudaSuccess) e = dalloc(&h->d_pout, 4);
   if (prm->precision == MDG_FP32_MIXED && prm->stage_atoms != 0) {
     a.stage_cap = prm->stage_atoms < 0 ? kStageDefault : prm->stage_atoms;
     const int nblk = blocks_for(cap, kStageBlock);
@@ -698,14 +932,20 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
 
 mdg_status mdg_destroy(mdg_handle *h) {
   if (!h) return MDG_ERR_INVALID_ARGUMENT;
-  for (auto &t : h->writers) t.join();
+  if (h->writer.joinable()) h->writer.join();
   cudaSetDevice(h->prm.device);
+  if (h->snap_q) cudaFreeHost(h->snap_q);
+  if (h->snap_v) cudaFreeHost(h->snap_v);
+  if (h->snap_t) cudaFreeHost(h->snap_t);
+  if (h->snap_done) cudaEventDestroy(h->snap_done);
   if (h->stream) cudaStreamSynchronize(h->stream);
   destroy_graph(h);
   free_arrays(h->a);
   if (h->d_flags) cudaFree(h->d_flags);
   if (h->d_sums) cudaFree(h->d_sums);
   if (h->d_tiles) cudaFree(h->d_tiles);
+  if (h->d_bar) cudaFree(h->d_bar);
+  if (h->d_pout) cudaFree(h->d_pout);
   if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -935,6 +1175,7 @@ mdg_status mdg_change_scale(mdg_handle *h, double alpha) {
   for (int d = 0; d < 3; d++) L[d] = h->prm.L[d] * alpha;  // MDManager::ChangeScale, src/mdmanager.cc:573-585
   Box nb = h->box;
   if (!box_geometry(nb, L, h->box.sl)) return fail(h, MDG_ERR_BOX_TOO_SMALL, "scaled box below 3 cells per axis");
+  if (!cells_packable(nb)) return fail(h, MDG_ERR_INVALID_ARGUMENT, "scaled box above 2047 x 2047 x 1023 cells");
   // the reference builds the list (wrapping the atoms into the box) before
   // scaling and again after it
   const int one = 1;
@@ -947,10 +1188,12 @@ mdg_status mdg_change_scale(mdg_handle *h, double alpha) {
   if (nb.ncell > h->cell_cap) {
     cudaFree(h->a.cell_count);
     cudaFree(h->a.cell_start);
+    cudaFree(h->a.xsub);
     cudaFree(h->d_tiles);
-    h->a.cell_count = h->a.cell_start = h->d_tiles = nullptr;
+    h->a.cell_count = h->a.cell_start = h->a.xsub = h->d_tiles = nullptr;
     CUDA_TRY(h, dalloc(&h->a.cell_count, nb.ncell));
     CUDA_TRY(h, dalloc(&h->a.cell_start, nb.ncell + 1));
+    CUDA_TRY(h, dalloc(&h->a.xsub, trim_table_size(nb)));
     CUDA_TRY(h, dalloc(&h->d_tiles, (size_t)blocks_for(nb.ncell, kScanBlock) + 1));
     h->cell_cap = nb.ncell;
   }
@@ -1054,6 +1297,7 @@ mdg_status mdg_calculate(mdg_handle *h, int nsteps) {
   if (nsteps < 0) return MDG_ERR_INVALID_ARGUMENT;
   if (h->n == 0 || nsteps == 0) return MDG_OK;
   CUDA_TRY(h, cudaSetDevice(h->prm.device));
+  if ((r = autotune(h))) return r;
   Status st;
   if ((r = read_status(h, &st))) return r;
   if (st.error) return translate_device_error(h, st);
@@ -1066,6 +1310,33 @@ mdg_status mdg_calculate(mdg_handle *h, int nsteps) {
       k_pack_half<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n, h->a.qfix);
       h->kernel_launches++;
       h->fix_buf = 0;
+    }
+    if (h->use_graphs && use_persistent(h)) {
+      // steps back to back in one launch until one needs the displacement
+      // check or a rebuild; that step runs as an ordinary step
+      while (left > 0) {
+        if (h->fix_buf < 0) {
+          k_pack_half<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n, h->a.qfix);
+          h->kernel_launches++;
+          h->fix_buf = 0;
+        }
+        int taken = 0;
+        const int want = (int)std::min<long long>(left, 1 << 30);
+        const int tpa = h->tpa > 0 ? h->tpa : 1;
+        if ((r = tpa == 4 ? launch_persistent<4>(h, want, &taken)
+                          : (tpa == 2 ? launch_persistent<2>(h, want, &taken) : launch_persistent<1>(h, want, &taken))))
+          return r;
+        left -= taken;
+        if (left > 0) {
+          if ((r = step_eager(h))) return r;
+          left--;
+        }
+        if ((r = read_status(h, &st))) return r;
+        if (st.error) {
+          left = 0;  // handled below (a row overflow grows the rows and redoes the rest)
+          break;
+        }
+      }
     }
     if (h->use_graphs && left >= kStepsPerGraph && h->graph_dirty) {
       if ((r = build_graph(h))) return r;
@@ -1211,6 +1482,10 @@ mdg_status mdg_get_info(mdg_handle *h, mdg_info *info) {
   info->displacement_checks = st.disp_checks;
   info->simulation_time = st.sim_time;
   info->buffer_left = st.budget;
+  info->threads_per_atom = h->tpa;
+  info->build_block = h->build_block;
+  info->build_threads_per_atom = h->build_tpa;
+  info->persistent_steps = h->persistent_steps;
   return MDG_OK;
 }
 
@@ -1415,37 +1690,56 @@ mdg_status mdg_load_checkpoint(mdg_handle *h, const char *path) {
 }
 
 // ------------------------------------------------------ snapshots
+namespace {
+// Joins the pending writer, if any; MDG_ERR_IO with its message if it failed.
+mdg_status join_writer(mdg_handle *h) {
+  if (h->writer.joinable()) h->writer.join();
+  if (!h->writer_error.empty()) {
+    const std::string msg = h->writer_error;
+    h->writer_error.clear();
+    return fail(h, MDG_ERR_IO, msg);
+  }
+  return MDG_OK;
+}
+}  // namespace
+
 mdg_status mdg_snapshot_async(mdg_handle *h, const char *path, int format) {
   mdg_status r = check_ready(h);
   if (r) return r;
   if (!path || (format != MDG_SNAPSHOT_CDVIEW && format != MDG_SNAPSHOT_CONFIGURATION))
     return MDG_ERR_INVALID_ARGUMENT;
+  // the previous file is finished (and its failure reported) before its
+  // buffers are reused
+  if ((r = join_writer(h))) return r;
   CUDA_TRY(h, cudaSetDevice(h->prm.device));
   const int n = h->n;
-  double4 *hq = nullptr, *hv = nullptr;
-  int *ht = nullptr;
-  CUDA_TRY(h, cudaHostAlloc((void **)&hq, sizeof(double4) * std::max(n, 1), cudaHostAllocDefault));
-  cudaError_t e = cudaHostAlloc((void **)&hv, sizeof(double4) * std::max(n, 1), cudaHostAllocDefault);
-  if (e == cudaSuccess) e = cudaHostAlloc((void **)&ht, sizeof(int) * std::max(n, 1), cudaHostAllocDefault);
-  cudaEvent_t done = nullptr;
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
-  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(hq, h->a.q, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(hv, h->a.v, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(ht, h->a.type, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess) e = cudaEventRecord(done, h->stream);
-  if (e != cudaSuccess) {
-    if (done) cudaEventDestroy(done);
-    cudaFreeHost(hq);
-    if (hv) cudaFreeHost(hv);
-    if (ht) cudaFreeHost(ht);
-    return fail(h, MDG_ERR_CUDA, std::string("snapshot copy: ") + cudaGetErrorString(e));
+  if (n > h->snap_cap || !h->snap_q) {
+    if (h->snap_q) cudaFreeHost(h->snap_q);
+    if (h->snap_v) cudaFreeHost(h->snap_v);
+    if (h->snap_t) cudaFreeHost(h->snap_t);
+    h->snap_q = h->snap_v = nullptr;
+    h->snap_t = nullptr;
+    h->snap_cap = 0;
+    const int cap = std::max(n, 1);
+    CUDA_TRY(h, cudaHostAlloc((void **)&h->snap_q, sizeof(double4) * cap, cudaHostAllocDefault));
+    CUDA_TRY(h, cudaHostAlloc((void **)&h->snap_v, sizeof(double4) * cap, cudaHostAllocDefault));
+    CUDA_TRY(h, cudaHostAlloc((void **)&h->snap_t, sizeof(int) * cap, cudaHostAllocDefault));
+    h->snap_cap = cap;
   }
+  if (!h->snap_done) CUDA_TRY(h, cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming));
+  if (n > 0) {
+    CUDA_TRY(h, cudaMemcpyAsync(h->snap_q, h->a.q, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->snap_v, h->a.v, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->snap_t, h->a.type, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CUDA_TRY(h, cudaEventRecord(h->snap_done, h->stream));
   const std::string file(path);
   const int dev = h->prm.device;
-  h->writers.emplace_back([h, file, format, n, hq, hv, ht, done, dev]() {
+  h->writer = std::thread([h, file, format, n, dev]() {
+    const double4 *hq = h->snap_q, *hv = h->snap_v;
+    const int *ht = h->snap_t;
     cudaSetDevice(dev);
-    const cudaError_t ce = cudaEventSynchronize(done);
-    bool ok = ce == cudaSuccess;
+    bool ok = cudaEventSynchronize(h->snap_done) == cudaSuccess;
     if (ok) {
       FILE *fp = fopen(file.c_str(), "w");
       ok = fp != nullptr;
@@ -1459,29 +1753,15 @@ mdg_status mdg_snapshot_async(mdg_handle *h, const char *path, int format) {
       }
       if (fp && fclose(fp) != 0) ok = false;
     }
-    cudaEventDestroy(done);
-    cudaFreeHost(hq);
-    cudaFreeHost(hv);
-    cudaFreeHost(ht);
-    if (!ok) {
-      std::lock_guard<std::mutex> lock(h->writer_mutex);
-      if (h->writer_error.empty()) h->writer_error = "snapshot not written: " + file;
-    }
+    // read by the joining thread only after join()
+    if (!ok) h->writer_error = "snapshot not written: " + file;
   });
   return MDG_OK;
 }
 
 mdg_status mdg_snapshot_wait(mdg_handle *h) {
   if (!h) return MDG_ERR_INVALID_ARGUMENT;
-  for (auto &t : h->writers) t.join();
-  h->writers.clear();
-  std::lock_guard<std::mutex> lock(h->writer_mutex);
-  if (!h->writer_error.empty()) {
-    const std::string msg = h->writer_error;
-    h->writer_error.clear();
-    return fail(h, MDG_ERR_IO, msg);
-  }
-  return MDG_OK;
+  return join_writer(h);
 }
 
 }  // extern "C"

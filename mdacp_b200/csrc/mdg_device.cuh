@@ -15,7 +15,16 @@
 //                            index up to a multiple of 4 (the FP32 force loop
 //                            walks 4 partners at a time; a self entry has r = 0
 //                            and is masked)
-//   qloc      float4[cap]    cell-local FP32 coordinates at the last build
+//   qloc      float4[cap]    FP32 coordinates at the last build for the list
+//                            prefilter: x in box coordinates, y and z
+//                            relative to the atom's cell
+//   cxyz      int32[cap]     the slot's cell coordinates at the last build,
+//                            packed x | y << 11 | z << 22
+//   xsub      int32[rows*(8*ms_x+1)]  list-build trim table, one block per
+//                            x-row of cells: atoms inside a cell are in x
+//                            order, entry 8*cx + k of a row's block is the first
+//                            slot of its cell cx at or beyond x0 + k cs_x / 8,
+//                            and entry 8*ms_x is the end of the row
 //   nbr16     uint2[maxnb/4][stride]  FP32-mixed only: the same rows as 16-bit
 //                            indices into the block's staged partner positions
 //                            (four per 8-byte load); see k_stage_plan
@@ -54,6 +63,13 @@ struct Box {
   int check_list_length;
   double cs[3];        // cell size L / ms
   float sl2_lo, sl2_hi;  // FP32 prefilter band around SearchLength^2
+  // z-slab of a decomposed system (slab = 1): the owned cell layers are the
+  // global layers z0 .. z0 + nzl - 1, and cell indices, packed cell
+  // coordinates and trim-table rows use the local layer z - z0; the trim
+  // table has two more blocks of rows, the ghost layers below (block nzl)
+  // and above (block nzl + 1).  A single domain has slab = 0, z0 = 0 and
+  // nzl = ms[2].
+  int slab, z0, nzl;
 };
 
 // Mutable device-side state of one handle.
@@ -95,7 +111,9 @@ struct Arrays {
   double4 *q, *v, *q_old;
   int4 *qfix;
   int4 *qfix2;        // second fixed-point buffer: the fused NVE step reads one and writes the other
-  float4 *qloc;       // cell-local FP32 coordinates at the last build (list prefilter)
+  float4 *qloc;       // FP32 coordinates at the last build (list prefilter): x global, y z cell-local
+  int *cxyz;          // packed cell coordinates of each slot at the last build
+  int *xsub;          // x sub-bin starts of every cell and row ends (list-build trim table)
   int *ids, *type;
   int *cell;          // cell of each slot at the last build
   int *nbr, *nnbr;
@@ -116,6 +134,19 @@ struct Arrays {
   uint2 *nbr16;       // rows as stage indices, four 16-bit entries per element
   int stage_cap;      // atoms one block stages at most
 };
+
+// The FP32 prefilter band of the list build: candidates whose FP32 r^2 lies
+// in [lo, hi] around SearchLength^2 are decided by the exact FP64 test.  The
+// prefilter's x coordinate is the box coordinate (error up to one rounding
+// of L_x) and y, z are cell-local, so with u = 2^-24 the FP32 r^2 of a
+// candidate near the search length is within u (6 L_x / SL + 37) SL^2 of
+// the exact value; the band is four times that, and at least 1e-4 SL^2.
+inline void prefilter_band(double sl2, double sl, double lx, float *lo, float *hi) {
+  const double u = 1.0 / 16777216.0;
+  const double rel = fmax(1e-4, 4.0 * u * (6.0 * lx / sl + 37.0));
+  *lo = (float)(sl2 * (1.0 - rel));
+  *hi = (float)(sl2 * (1.0 + rel));
+}
 
 // ------------------------------------------------------------------ helpers
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
@@ -583,6 +614,67 @@ __global__ void __launch_bounds__(BLOCK) k_stage_plan(Arrays a, Box b, int n) {
   a.stage_n[blk] = over ? -1 : m;
 }
 
+// ------------------------------------------------------------- list build
+// x sub-bins per cell of the list build's trim table (see xsub above).
+constexpr int kXSub = 8;
+
+// Cell coordinates packed into one int (x and y below 2048, z below 1024).
+__device__ __forceinline__ int pack_cell(int cx, int cy, int cz) { return cx | (cy << 11) | (cz << 22); }
+
+// Trim-table entries of a cell: the block of its x-row, at its x position.
+__device__ __forceinline__ int *trim_entries(int *tab, int ms0, int row, int cx) {
+  return tab + (size_t)row * (ms0 * kXSub + 1) + cx * kXSub;
+}
+
+// One warp orders the cnt slots perm[beg, beg + cnt) of a cell by (x, upload
+// id) into perm2 and writes the cell's entries of the trim table: ent[k] =
+// beg + (atoms with x < x0 + k bin), k < kXSub, and for the last cell of a
+// row (last) the row's end ent[kXSub] = beg + cnt.  Ties in x (a lattice) go
+// by id, so the order is a function of the state alone.
+__device__ __forceinline__ void sort_cell_x(const double4 *q, const int *ids, const int *perm, int *perm2, int beg,
+                                            int cnt, double x0, double bin, int *ent, bool last, int lane) {
+  int below[kXSub];
+#pragma unroll
+  for (int k = 0; k < kXSub; k++) below[k] = 0;
+  for (int base = 0; base < cnt; base += 32) {
+    const int me = base + lane;
+    int my_slot = -1, my_id = 0x7fffffff;
+    double my_x = 0.0;
+    if (me < cnt) {
+      my_slot = perm[beg + me];
+      my_x = q[my_slot].x;
+      my_id = ids[my_slot];
+    }
+    int rank = 0;
+    for (int ob = 0; ob < cnt; ob += 32) {
+      const int other = ob + lane;
+      double ox = 0.0;
+      int oid = 0x7fffffff;
+      if (other < cnt) {
+        const int os = perm[beg + other];
+        ox = q[os].x;
+        oid = ids[os];
+      }
+      const int lim = min(32, cnt - ob);
+      for (int k = 0; k < lim; k++) {
+        const double kx = __shfl_sync(0xffffffffu, ox, k);
+        const int kid = __shfl_sync(0xffffffffu, oid, k);
+        rank += (kx < my_x || (kx == my_x && kid < my_id)) ? 1 : 0;
+      }
+    }
+    if (me < cnt) perm2[beg + rank] = my_slot;
+#pragma unroll
+    for (int k = 1; k < kXSub; k++)
+      below[k] += __popc(__ballot_sync(0xffffffffu, me < cnt && my_x < x0 + k * bin));
+  }
+  int v = 0;
+#pragma unroll
+  for (int k = 1; k < kXSub; k++)
+    if (lane == k) v = below[k];
+  if (lane < kXSub) ent[lane] = beg + v;
+  if (last && lane == 0) ent[kXSub] = beg + cnt;
+}
+
 // Rebuild 1/6: wrap into [0,L] (Variables::AdjustPeriodicBoundary,
 // src/variables.cc:63-84), validity check, cell index and rank inside the cell.
 template <int BLOCK>
@@ -610,6 +702,13 @@ __global__ void __launch_bounds__(BLOCK) k_cell_assign(Arrays a, Box b, int n) {
   }
   q.x = x[0]; q.y = x[1]; q.z = x[2];
   a.q[i] = q;
+  if (b.slab) {  // the slab's own layers only (migration moved every other atom away)
+    cc[2] -= b.z0;
+    if (cc[2] < 0 || cc[2] >= b.nzl) {
+      atomicOr(&a.st->error, kErrInvalidPosition);
+      return;
+    }
+  }
   const int c = (cc[2] * b.ms[1] + cc[1]) * b.ms[0] + cc[0];
   a.cell[i] = c;
   a.slot[i] = atomicAdd(&a.cell_count[c], 1);
@@ -689,32 +788,18 @@ __global__ void __launch_bounds__(BLOCK) k_scatter(Arrays a, int n) {
   a.perm[a.cell_start[a.cell[i]] + a.slot[i]] = i;
 }
 
-// Rebuild 4/6: order every cell by upload id (one warp per cell), which makes
-// the slot order a function of the state alone, independent of atomics.
-static __global__ void k_sort_cells(Arrays a, int ncell) {
+// Rebuild 4/6: order every cell by (x, upload id), one warp per cell, which
+// makes the slot order a function of the state alone (independent of
+// atomics) and puts each cell's atoms in x order for the list build's trim
+// table; the cell's row of that table is written too (sort_cell_x).
+static __global__ void k_sort_cells(Arrays a, Box b, int ncell) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= ncell || a.st->error) return;
   const int beg = a.cell_start[warp], cnt = a.cell_start[warp + 1] - beg;
-  for (int base = 0; base < cnt; base += 32) {
-    const int me = base + lane;
-    int my_slot = -1, my_key = 0x7fffffff;
-    if (me < cnt) {
-      my_slot = a.perm[beg + me];
-      my_key = a.ids[my_slot];
-    }
-    int rank = 0;
-    for (int ob = 0; ob < cnt; ob += 32) {
-      const int other = ob + lane;
-      int okey = 0x7fffffff;
-      if (other < cnt) okey = a.ids[a.perm[beg + other]];
-      for (int k = 0; k < 32; k++) {
-        const int kk = __shfl_sync(0xffffffffu, okey, k);
-        if (ob + k < cnt && kk < my_key) rank++;
-      }
-    }
-    if (me < cnt) a.perm2[beg + rank] = my_slot;
-  }
+  const int cx = warp % b.ms[0];
+  sort_cell_x(a.q, a.ids, a.perm, a.perm2, beg, cnt, cx * b.cs[0], b.cs[0] / kXSub,
+              trim_entries(a.xsub, b.ms[0], warp / b.ms[0], cx), cx == b.ms[0] - 1, lane);
 }
 
 // Ghost-strip membership of a wrapped position at a build: bit 2d for
@@ -751,11 +836,13 @@ __global__ void __launch_bounds__(BLOCK) k_permute(Arrays a, Box b, int n, int4 
     a.q_old[s] = q;
     const double x[3] = {q.x, q.y, q.z};
     a.mult[s] = (unsigned char)border_bits(x, b, &m);
-    // cell-local FP32 coordinates for the list prefilter
+    // FP32 coordinates for the list prefilter (x in box coordinates, y and z
+    // relative to the cell) and the packed cell coordinates
     const int c = a.cell_tmp[s];
     const int cx = c % b.ms[0], cy = (c / b.ms[0]) % b.ms[1], cz = c / (b.ms[0] * b.ms[1]);
-    a.qloc[s] = make_float4((float)(q.x - cx * b.cs[0]), (float)(q.y - cy * b.cs[1]),
-                            (float)(q.z - cz * b.cs[2]), 0.f);
+    const int gz = cz + b.z0;  // global layer (the local one in a slab)
+    a.qloc[s] = make_float4((float)q.x, (float)(q.y - cy * b.cs[1]), (float)(q.z - gz * b.cs[2]), 0.f);
+    a.cxyz[s] = pack_cell(cx, cy, cz);
     if (pack) {
       // the coming step's first-drift positions for the fused FP32 NVE pass
       const double4 v = a.v[o];
@@ -792,18 +879,181 @@ __device__ __forceinline__ bool within_search_exact(const double4 &qi, const dou
   return !(r2 > sl2);
 }
 
-// Rebuild 6/6: full Verlet list.  One thread per atom walks the 27 cells
-// around its own (periodic, >= 3 cells per axis so they are distinct).  Each
-// candidate is first tested in FP32 on cell-local coordinates (one FADD per
-// axis: the neighbour cell's offset is folded into a per-cell base); only
-// candidates whose FP32 r^2 falls in a thin band around SearchLength^2 --
-// wider than the FP32 error by a factor of about 40 -- are decided by the
-// exact FP64 test, so the pair set is the reference's bit for bit.  Row
-// order: cells in (dz,dy,dx) order, slots ascending; rows padded with the
+// Candidates [beg, end) of one stencil row of atom i, in slot order: FP32
+// prefilter r^2 <= hi on the prefilter coordinates moved by the row's base
+// (bx, by, bz); the ghost-existence rule for image shifts (NEED); the exact
+// FP64 test for candidates in the band [lo, hi]; emit(j, k) files partner j
+// as entry k of the row.  SELF: the range holds atom i itself.  Four loads
+// are issued before the first test.
+//
+// With BTPA lanes per atom (the lanes of one atom are consecutive and all
+// walk the same ranges), lane s tests candidates beg + s, beg + BTPA + s, ...
+// and the lanes file the ones they keep in slot order through a ballot over
+// the atom's lanes, so the row is the same for every lane count; cnt stays
+// equal on all of them.
+template <bool NEED, bool SELF, int BTPA, typename Emit>
+__device__ __forceinline__ void build_range(const float4 *__restrict__ qloc, const double4 *__restrict__ q,
+                                            const unsigned char *__restrict__ mult, int beg, int end, float bx,
+                                            float by, float bz, int need, double sx, double sy, double sz, int i,
+                                            const double4 &qi, float lo, float hi, double sl2, int &cnt,
+                                            Emit &emit) {
+  auto keep_of = [&](int j, const float4 &l) {
+    const float ex = l.x + bx, ey = l.y + by, ez = l.z + bz;
+    const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+    bool keep = r2 <= hi;
+    if (SELF) keep = keep && j != i;
+    if (NEED) keep = keep && (mult[j] & need) == need;
+    if (keep && r2 >= lo) keep = within_search_exact(qi, q[j], sx, sy, sz, sl2);
+    return keep;
+  };
+  if (BTPA == 1) {
+    auto test = [&](int j, const float4 &l) {
+      if (keep_of(j, l)) {
+        emit(j, cnt);
+        cnt++;
+      }
+    };
+    int j = beg;
+    for (; j + 4 <= end; j += 4) {
+      const float4 l0 = __ldg(qloc + j), l1 = __ldg(qloc + j + 1), l2 = __ldg(qloc + j + 2),
+                   l3 = __ldg(qloc + j + 3);
+      test(j, l0);
+      test(j + 1, l1);
+      test(j + 2, l2);
+      test(j + 3, l3);
+    }
+    for (; j < end; j++) test(j, __ldg(qloc + j));
+  } else {
+    const int lane = threadIdx.x & 31, sub = lane & (BTPA - 1), first = lane & ~(BTPA - 1);
+    const unsigned gmask = (BTPA == 32) ? 0xffffffffu : (((1u << BTPA) - 1u) << first);
+    const unsigned below = (1u << sub) - 1u;
+    auto file = [&](int j, bool keep) {
+      const unsigned m = __ballot_sync(gmask, keep) >> first;
+      if (keep) emit(j, cnt + __popc(m & below));
+      cnt += __popc(m);
+    };
+    for (int base = beg; base < end; base += 2 * BTPA) {
+      const int j0 = base + sub, j1 = base + BTPA + sub;
+      float4 l0 = make_float4(0.f, 0.f, 0.f, 0.f), l1 = l0;
+      if (j0 < end) l0 = __ldg(qloc + j0);
+      if (j1 < end) l1 = __ldg(qloc + j1);
+      const bool k0 = j0 < end && keep_of(j0, l0);
+      const bool k1 = j1 < end && keep_of(j1, l1);
+      file(j0, k0);
+      file(j1, k1);
+    }
+  }
+}
+
+// The full Verlet row of atom i (MeshList::SearchMesh's pair set, src/
+// meshlist.cc:242-292, seen from i): the 27 cells around i's own cell
+// (periodic, >= 3 cells per axis so they are distinct) are walked as 9 rows
+// along x.  Cells of a row are consecutive in slot order and atoms inside a
+// cell are in x order, so one row is one contiguous slot range (two or
+// three where the periodic wrap splits it), trimmed at both ends through the
+// trim table to the sub-bins that reach within SearchLength of x_i; rows
+// whose y-z gap to i already exceeds SearchLength are skipped.  Row order:
+// rows in (dz, dy) order, then x order across the row's cells -- the cells
+// in dx order, as a 27-cell walk visits them.  Returns the partners found
+// (entries beyond the capacity are counted, not filed).
+template <bool SLAB = false, int BTPA = 1, typename Emit>
+__device__ __forceinline__ int build_rows(const Box &b, const float4 *__restrict__ qloc,
+                                          const double4 *__restrict__ q, const unsigned char *__restrict__ mult,
+                                          const int *__restrict__ tab, int pc, int i, Emit &emit) {
+  const float4 li = qloc[i];
+  const double4 qi = q[i];
+  const int cx = pc & 2047, cy = (pc >> 11) & 2047, lz = pc >> 22;
+  const int cz = SLAB ? b.z0 + lz : lz;  // global layer
+  const int ms0 = b.ms[0], ms1 = b.ms[1], ms2 = b.ms[2];
+  const float lo = b.sl2_lo, hi = b.sl2_hi;
+  // sub-bins [vlo, vhi) of the virtual row of cells cx-1 .. cx+1 (unwrapped
+  // x) that can hold a partner: every bin that reaches [x_i - SL, x_i + SL]
+  const double cs0 = b.cs[0], per_bin = kXSub / cs0;
+  int vlo = (cx - 1) * kXSub + (int)floor((qi.x - (cx - 1) * cs0 - b.sl) * per_bin - 1e-6);
+  int vhi = (cx + 1) * kXSub + (int)floor((qi.x - (cx + 1) * cs0 + b.sl) * per_bin + 1e-6) + 1;
+  vlo = max(vlo, (cx - 1) * kXSub);
+  vhi = min(vhi, (cx + 2) * kXSub);
+  const int mx = ms0 * kXSub;
+  const float csy = (float)b.cs[1], csz = (float)b.cs[2];
+  // x bases of the three pieces (image shifts -L, 0, +L); prefilter x is global
+  const float bxm = (float)(-b.L[0] - qi.x), bx0 = (float)(-qi.x), bxp = (float)(b.L[0] - qi.x);
+  int cnt = 0;
+  for (int dz = -1; dz <= 1; dz++) {
+    int z = cz + dz;
+    double sz = 0.0;
+    if (z < 0) { z += ms2; sz = -b.L[2]; } else if (z >= ms2) { z -= ms2; sz = b.L[2]; }
+    const float bz = (float)((z - cz) * b.cs[2] + sz) - li.z;
+    const float gz = dz == 0 ? 0.f : (dz < 0 ? li.z : csz - li.z);
+    // the layer's block of trim-table rows: the global layer in a single
+    // domain; in a slab an owned local layer or one of the two ghost blocks
+    int blk = z;
+    if (SLAB) {
+      const int nl = lz + dz;
+      blk = nl < 0 ? b.nzl : (nl >= b.nzl ? b.nzl + 1 : nl);
+    }
+    for (int dy = -1; dy <= 1; dy++) {
+      const float gy = dy == 0 ? 0.f : (dy < 0 ? li.y : csy - li.y);
+      if (fmaf(gy, gy, gz * gz) > hi) continue;  // the whole row is out of reach
+      int y = cy + dy;
+      double sy = 0.0;
+      if (y < 0) { y += ms1; sy = -b.L[1]; } else if (y >= ms1) { y -= ms1; sy = b.L[1]; }
+      const float by = (float)((y - cy) * b.cs[1] + sy) - li.y;
+      const int *xr = tab + (size_t)(blk * ms1 + y) * (mx + 1);
+      if (vlo < 0) {  // through the -x face: the row's last cells, image shift -L
+        const double sx = -b.L[0];
+        const int need = needed_strips(sx, sy, sz);
+        build_range<true, false, BTPA>(qloc, q, mult, xr[vlo + mx], xr[mx], bxm, by, bz, need, sx, sy, sz, i, qi, lo, hi,
+                                 b.sl2, cnt, emit);
+      }
+      {
+        const int a0 = max(vlo, 0), a1 = min(vhi, mx);
+        const int beg = xr[a0], end = xr[a1];
+        const int need = needed_strips(0.0, sy, sz);
+        if (dz == 0 && dy == 0)
+          build_range<false, true, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, 0, 0.0, sy, sz, i, qi, lo, hi, b.sl2, cnt,
+                                   emit);
+        else if (need)
+          build_range<true, false, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, need, 0.0, sy, sz, i, qi, lo, hi, b.sl2,
+                                   cnt, emit);
+        else
+          build_range<false, false, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, 0, 0.0, sy, sz, i, qi, lo, hi, b.sl2, cnt,
+                                    emit);
+      }
+      if (vhi > mx) {  // through the +x face: the row's first cells, image shift +L
+        const double sx = b.L[0];
+        const int need = needed_strips(sx, sy, sz);
+        build_range<true, false, BTPA>(qloc, q, mult, xr[0], xr[vhi - mx], bxp, by, bz, need, sx, sy, sz, i, qi, lo, hi,
+                                 b.sl2, cnt, emit);
+      }
+    }
+  }
+  return cnt;
+}
+
+// Stage offset of global slot j: the plan range whose atoms hold j (ranges
+// are sorted by first cell, so by first atom).
+__device__ __forceinline__ int stage_shift_atom(const int4 *plan, int npl, int j) {
+  int lo = 0, hi = npl - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (plan[mid].z <= j) lo = mid;
+    else hi = mid - 1;
+  }
+  return plan[lo].w - plan[lo].z;
+}
+
+// Rebuild 6/6: full Verlet list, one thread per atom (build_rows).  Each
+// candidate is first tested in FP32; only candidates whose FP32 r^2 falls in
+// a band around SearchLength^2 -- wider than the FP32 error bound, which
+// mdg_create derives from the box -- are decided by the exact FP64 test, so
+// the pair set is the reference's bit for bit.  Rows are padded with the
 // atom's own index to a multiple of 4.
-template <int BLOCK, bool STAGE>
+template <int BLOCK, bool STAGE, bool SLAB = false, int BTPA = 1>
 __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
-  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  static_assert(!(STAGE && SLAB), "staged rows are single-domain only");
+  static_assert(!STAGE || BTPA == 1, "staged rows are built one lane per atom");
+  const int t = blockIdx.x * BLOCK + threadIdx.x;
+  const int i = t / BTPA, sub = t % BTPA;
   int cnt = 0;
   // STAGE: also the rows as stage indices (FP32-mixed staged force), from
   // the block's stage plan, see k_stage_plan
@@ -831,81 +1081,43 @@ __global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
     staged_atoms = npl > 0 ? nstaged : 0;
   }
   unsigned g0 = 0u, g1 = 0u;  // the row's current group of four stage indices
-  if (i < n && !a.st->error) {
-    const float4 li = a.qloc[i];
-    const int c = a.cell_tmp[i];
-    const int cx = c % b.ms[0], cy = (c / b.ms[0]) % b.ms[1], cz = c / (b.ms[0] * b.ms[1]);
+  // one decision per atom: the lanes of an atom must walk its rows together
+  // (their ballots name each other), so they all see its first lane's read
+  // of the error flag
+  int err = a.st->error;
+  if (BTPA > 1) err = __shfl_sync(0xffffffffu, err, (threadIdx.x & 31) & ~(BTPA - 1));
+  if (i < n && !err) {
     const int maxnb = a.maxnb, stride = a.stride;
-    const float lo = b.sl2_lo, hi = b.sl2_hi;
-    for (int dz = -1; dz <= 1; dz++) {
-      int z = cz + dz;
-      double sz = 0.0;
-      if (z < 0) { z += b.ms[2]; sz = -b.L[2]; } else if (z >= b.ms[2]) { z -= b.ms[2]; sz = b.L[2]; }
-      const float bz = (float)((z - cz) * b.cs[2] + sz) - li.z;
-      for (int dy = -1; dy <= 1; dy++) {
-        int y = cy + dy;
-        double sy = 0.0;
-        if (y < 0) { y += b.ms[1]; sy = -b.L[1]; } else if (y >= b.ms[1]) { y -= b.ms[1]; sy = b.L[1]; }
-        const float by = (float)((y - cy) * b.cs[1] + sy) - li.y;
-        for (int dx = -1; dx <= 1; dx++) {
-          int x = cx + dx;
-          double sx = 0.0;
-          if (x < 0) { x += b.ms[0]; sx = -b.L[0]; } else if (x >= b.ms[0]) { x -= b.ms[0]; sx = b.L[0]; }
-          const float bx = (float)((x - cx) * b.cs[0] + sx) - li.x;
-          const int nc = (z * b.ms[1] + y) * b.ms[0] + x;
-          const int beg = a.cell_start[nc], end = a.cell_start[nc + 1];
-          const int need = needed_strips(sx, sy, sz);
-          const int shift = (STAGE && npl > 0) ? stage_shift(plan, npl, nc) : 0;
-          // one candidate, in row order (FP32 prefilter, ghost rule, exact band)
-          auto accept = [&](int j, float r2) {
-            if (r2 > hi || j == i) return;
-            if (need && (a.mult[j] & need) != need) return;
-            if (r2 >= lo && !within_search_exact(a.q[i], a.q[j], sx, sy, sz, b.sl2)) return;
-            if (cnt < maxnb) {
-              a.nbr[(size_t)cnt * stride + i] = j;
-              if (STAGE && npl > 0) {
-                int v = j + shift;
-                if (v < 0 || v >= staged_atoms) {
-                  atomicOr(&a.st->error, kErrStage);
-                  v = 0;
-                }
-                stage_entry(a.nbr16, stride, i, cnt, v, g0, g1);
-              }
-            }
-            cnt++;
-          };
-          auto dist2f = [&](const float4 &lj) {
-            const float ex = lj.x + bx, ey = lj.y + by, ez = lj.z + bz;
-            return fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-          };
-          // two candidates per iteration: both loads issue before either
-          // test (the loop is bound by their latency)
-          int j = beg;
-          for (; j + 1 < end; j += 2) {
-            const float4 l0 = a.qloc[j], l1 = a.qloc[j + 1];
-            const float r0 = dist2f(l0), r1 = dist2f(l1);
-            accept(j, r0);
-            accept(j + 1, r1);
-          }
-          if (j < end) accept(j, dist2f(a.qloc[j]));
+    int *__restrict__ nbr = a.nbr;
+    auto emit = [&](int j, int k) {
+      if (k >= maxnb) return;
+      nbr[(size_t)k * stride + i] = j;
+      if (STAGE && npl > 0) {
+        int v = j + stage_shift_atom(plan, npl, j);
+        if (v < 0 || v >= staged_atoms) {
+          atomicOr(&a.st->error, kErrStage);
+          v = 0;
         }
+        stage_entry(a.nbr16, stride, i, k, v, g0, g1);
       }
-    }
-    a.nnbr[i] = min(cnt, maxnb);
+    };
+    cnt = build_rows<SLAB, BTPA>(b, a.qloc, a.q, a.mult, a.xsub, a.cxyz[i], i, emit);
+    if (sub == 0) a.nnbr[i] = min(cnt, maxnb);
     if (cnt > maxnb) {
-      atomicOr(&a.st->error, kErrCapacity);
-    } else {
-      int self = (STAGE && npl > 0) ? i + stage_shift(plan, npl, c) : 0;
+      if (sub == 0) atomicOr(&a.st->error, kErrCapacity);
+    } else if (sub == 0) {
+      int self = (STAGE && npl > 0) ? i + stage_shift(plan, npl, a.cell_tmp[i]) : 0;
       if (STAGE && npl > 0 && (self < 0 || self >= staged_atoms)) {
         atomicOr(&a.st->error, kErrStage);
         self = 0;
       }
       for (int k = cnt; k < ((cnt + 3) & ~3); k++) {
-        a.nbr[(size_t)k * stride + i] = i;
+        nbr[(size_t)k * stride + i] = i;
         if (STAGE && npl > 0) stage_entry(a.nbr16, stride, i, k, self, g0, g1);
       }
     }
   }
+  if (sub != 0) cnt = 0;  // the atom's row is counted once
   const int wmax = __reduce_max_sync(0xffffffffu, cnt);
   const int wsum = __reduce_add_sync(0xffffffffu, cnt);
   if ((threadIdx.x & 31) == 0 && wsum) {
@@ -1257,115 +1469,169 @@ __device__ __forceinline__ void fp32_finish(Arrays &a, const Box &b, const Therm
   }
 }
 
-// Row sum of atom i from the global fixed-point copy: rows are padded to a
-// multiple of 4, so the row is walked four partners at a time without
-// per-lane masks, with the indices of the next eight partners already in
-// flight (the list is the one stream from HBM, so its loads are issued two
-// groups ahead); FP32 partial sums over 8 partners are folded into the FP64
-// sums.
-__device__ __forceinline__ void fp32_row_global(const Arrays &a, const Box &b, const int4 *qf, int i,
-                                                const int4 &pi, int nn4, double &Fx, double &Fy, double &Fz) {
-  const float sx = b.fix_scale[0], sy = b.fix_scale[1], sz = b.fix_scale[2];
-  const unsigned rc2_bits = __float_as_uint(b.rc2f);
-  const float c2x8 = b.c2x8f;
-  const int *row = a.nbr + i;
-  const int st = a.stride;
-  float fx = 0.f, fy = 0.f, fz = 0.f;
-  int n0 = i, n1 = i, n2 = i, n3 = i;
-  int m0 = i, m1 = i, m2 = i, m3 = i;
-  if (nn4 > 0) {
-    n0 = __ldg(row);
-    n1 = __ldg(row + st);
-    n2 = __ldg(row + 2 * st);
-    n3 = __ldg(row + 3 * st);
+// ------------------------------------------------ FP32 row sums, 1-4 lanes per atom
+// The row sum of an atom in a fixed order that does not depend on how many
+// lanes share the row, so that 1, 2 or 4 lanes per atom give bit-identical
+// forces: the row's G groups of four entries (rows are padded to a multiple
+// of 4 with masked self entries) are split into four quarters of
+// Q = ceil(G / 4) consecutive groups; inside a quarter the pair terms are
+// summed in FP32 over two groups (8 partners) at a time, in entry order, and
+// folded into the quarter's FP64 sum S_t; the row sum is
+// (S0 + S1) + (S2 + S3).  With TPA lanes per atom, lane s sums quarters
+// s*4/TPA .. (s+1)*4/TPA - 1 and the lanes combine by butterfly shuffles,
+// which form exactly that tree.
+
+// Partner positions of a lane's groups from the global fixed-point copy:
+// the four list entries of the next group are in flight while a group is
+// summed (the list is the one stream from HBM, so its loads run ahead).
+struct GlobalGroups {
+  const int *row;  // nbr + atom
+  int st;          // list stride
+  const int4 *qf;
+  int self;
+  int n0, n1, n2, n3, m0, m1, m2, m3;
+  __device__ __forceinline__ void load(int g, int &x0, int &x1, int &x2, int &x3) const {
+    const int *r = row + (size_t)(4 * g) * st;
+    x0 = __ldg(r);
+    x1 = __ldg(r + st);
+    x2 = __ldg(r + 2 * st);
+    x3 = __ldg(r + 3 * st);
   }
-  if (nn4 > 4) {
-    m0 = __ldg(row + 4 * st);
-    m1 = __ldg(row + 5 * st);
-    m2 = __ldg(row + 6 * st);
-    m3 = __ldg(row + 7 * st);
+  __device__ __forceinline__ void start(int g, int gend) {
+    n0 = n1 = n2 = n3 = m0 = m1 = m2 = m3 = self;
+    if (g < gend) load(g, n0, n1, n2, n3);
+    if (g + 1 < gend) load(g + 1, m0, m1, m2, m3);
   }
-  for (int k = 0; k < nn4; k += 4) {
-    const int4 p0 = __ldg(qf + n0);
-    const int4 p1 = __ldg(qf + n1);
-    const int4 p2 = __ldg(qf + n2);
-    const int4 p3 = __ldg(qf + n3);
+  __device__ __forceinline__ void take(int g, int gend, int4 &p0, int4 &p1, int4 &p2, int4 &p3) {
+    p0 = __ldg(qf + n0);
+    p1 = __ldg(qf + n1);
+    p2 = __ldg(qf + n2);
+    p3 = __ldg(qf + n3);
     n0 = m0;
     n1 = m1;
     n2 = m2;
     n3 = m3;
-    if (k + 8 < nn4) {
-      const int *r = row + (size_t)(k + 8) * st;
-      m0 = __ldg(r);
-      m1 = __ldg(r + st);
-      m2 = __ldg(r + 2 * st);
-      m3 = __ldg(r + 3 * st);
-    }
-    lj_pair_fp32(pi, p0, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-    lj_pair_fp32(pi, p1, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-    lj_pair_fp32(pi, p2, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-    lj_pair_fp32(pi, p3, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-    if (k & 4) {
-      Fx += (double)fx;
-      Fy += (double)fy;
-      Fz += (double)fz;
-      fx = fy = fz = 0.f;
-    }
+    if (g + 2 < gend) load(g + 2, m0, m1, m2, m3);
   }
-  Fx += (double)fx;
-  Fy += (double)fy;
-  Fz += (double)fz;
-}
+};
 
-// The same row sum from the block's stage in shared memory: one 8-byte load
-// brings four stage indices; the next two groups are in flight.
+// The same from the block's stage in shared memory: one 8-byte load brings
+// four 16-bit stage indices; indices outside the stage are flagged and read
+// as entry 0.
 __device__ __forceinline__ unsigned stage_index(unsigned v, unsigned nstage, bool &bad) {
   const bool out = v >= nstage;
   bad |= out;
   return out ? 0u : v;
 }
 
-__device__ __forceinline__ void fp32_row_staged(const Arrays &a, const Box &b, const int4 *pos, unsigned nstage,
-                                                int i, const int4 &pi, int nn4, double &Fx, double &Fy,
-                                                double &Fz) {
-  const float sx = b.fix_scale[0], sy = b.fix_scale[1], sz = b.fix_scale[2];
-  const unsigned rc2_bits = __float_as_uint(b.rc2f);
-  const float c2x8 = b.c2x8f;
-  const uint2 *row = a.nbr16 + i;
-  const int st = a.stride;
-  float fx = 0.f, fy = 0.f, fz = 0.f;
-  uint2 g = make_uint2(0u, 0u), gn = make_uint2(0u, 0u);
-  bool bad = false;  // an index outside the stage: flagged, the read skipped
-  if (nn4 > 0) g = __ldg(row);
-  if (nn4 > 4) gn = __ldg(row + st);
-  for (int k = 0; k < nn4; k += 4) {
-    const int4 p0 = pos[stage_index(g.x & 0xffffu, nstage, bad)];
-    const int4 p1 = pos[stage_index(g.x >> 16, nstage, bad)];
-    const int4 p2 = pos[stage_index(g.y & 0xffffu, nstage, bad)];
-    const int4 p3 = pos[stage_index(g.y >> 16, nstage, bad)];
-    g = gn;
-    if (k + 8 < nn4) gn = __ldg(row + (size_t)((k + 8) >> 2) * st);
-    lj_pair_fp32(pi, p0, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-    lj_pair_fp32(pi, p1, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-    lj_pair_fp32(pi, p2, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-    lj_pair_fp32(pi, p3, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-    if (k & 4) {
-      Fx += (double)fx;
-      Fy += (double)fy;
-      Fz += (double)fz;
-      fx = fy = fz = 0.f;
-    }
+struct StagedGroups {
+  const uint2 *row;  // nbr16 + atom
+  int st;
+  const int4 *pos;   // the stage
+  unsigned nstage;
+  bool bad;
+  uint2 g0, g1;
+  __device__ __forceinline__ void start(int g, int gend) {
+    bad = false;
+    g0 = g1 = make_uint2(0u, 0u);
+    if (g < gend) g0 = __ldg(row + (size_t)g * st);
+    if (g + 1 < gend) g1 = __ldg(row + (size_t)(g + 1) * st);
   }
-  Fx += (double)fx;
-  Fy += (double)fy;
-  Fz += (double)fz;
-  if (bad) atomicOr(&a.st->error, kErrStage);
+  __device__ __forceinline__ void take(int g, int gend, int4 &p0, int4 &p1, int4 &p2, int4 &p3) {
+    p0 = pos[stage_index(g0.x & 0xffffu, nstage, bad)];
+    p1 = pos[stage_index(g0.x >> 16, nstage, bad)];
+    p2 = pos[stage_index(g0.y & 0xffffu, nstage, bad)];
+    p3 = pos[stage_index(g0.y >> 16, nstage, bad)];
+    g0 = g1;
+    if (g + 2 < gend) g1 = __ldg(row + (size_t)(g + 2) * st);
+  }
+};
+
+// Fixed-point scales and force constants of the FP32 pair term.
+struct PairConst {
+  float sx, sy, sz;
+  unsigned rc2_bits;
+  float c2x8;
+};
+
+__device__ __forceinline__ PairConst pair_const(const float fix_scale[3], float rc2f, float c2x8f) {
+  return PairConst{fix_scale[0], fix_scale[1], fix_scale[2], __float_as_uint(rc2f), c2x8f};
 }
 
-// FP32-mixed force kick.  Displacements come from the fixed-point copy (no
-// ghost atoms, no shift codes); the row sum is fp32_row_global's and the
-// kick is FP64.  With DRIFT the second half drift q += v dt/2 and the |v|
-// maximum of the step are done in the same pass: this kernel reads only the
+// Lane `sub` (of TPA) of a row of G groups: its quarters' part of the sum
+// tree (see above); all TPA lanes must call, and after
+// combine_lanes<TPA> every lane of the atom holds the row sum.
+template <int TPA, typename Groups>
+__device__ __forceinline__ void fp32_row_part(Groups &f, int G, int sub, const int4 &pi, const PairConst &k,
+                                              double &Fx, double &Fy, double &Fz) {
+  static_assert(TPA == 1 || TPA == 2 || TPA == 4, "1, 2 or 4 lanes per atom");
+  constexpr int QPL = 4 / TPA;  // quarters per lane
+  const int Q = (G + 3) >> 2;
+  const int q0 = sub * QPL;
+  const int gbeg = min(G, q0 * Q), gend = min(G, (q0 + QPL) * Q);
+  double Sx = 0.0, Sy = 0.0, Sz = 0.0, Px = 0.0, Py = 0.0, Pz = 0.0, Ax = 0.0, Ay = 0.0, Az = 0.0;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  int qidx = q0, gq = 0;
+  auto close_quarter = [&]() {
+    if (TPA == 4 || (qidx & 1) == 0) {
+      Px = Sx; Py = Sy; Pz = Sz;
+    } else {
+      Px = Px + Sx; Py = Py + Sy; Pz = Pz + Sz;
+    }
+    if (TPA == 1 && qidx == 1) {
+      Ax = Px; Ay = Py; Az = Pz;
+    }
+    Sx = Sy = Sz = 0.0;
+    qidx++;
+  };
+  f.start(gbeg, gend);
+  for (int g = gbeg; g < gend; g++) {
+    int4 p0, p1, p2, p3;
+    f.take(g, gend, p0, p1, p2, p3);
+    lj_pair_fp32(pi, p0, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
+    lj_pair_fp32(pi, p1, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
+    lj_pair_fp32(pi, p2, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
+    lj_pair_fp32(pi, p3, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
+    gq++;
+    const bool qend = gq == Q || g + 1 == gend;
+    if ((gq & 1) == 0 || qend) {
+      Sx += (double)fx;
+      Sy += (double)fy;
+      Sz += (double)fz;
+      fx = fy = fz = 0.f;
+    }
+    if (qend) {
+      close_quarter();
+      gq = 0;
+    }
+  }
+  while (qidx < q0 + QPL) close_quarter();  // quarters without groups: S_t = 0
+  if (TPA == 1) {
+    Fx = Ax + Px; Fy = Ay + Py; Fz = Az + Pz;
+  } else {
+    Fx = Px; Fy = Py; Fz = Pz;
+  }
+}
+
+// Butterfly over the TPA lanes of an atom: lane pairs (0,1), (2,3) first,
+// then the two pairs -- the (S0 + S1) + (S2 + S3) tree (IEEE addition is
+// commutative, so both lanes of a pair hold the same value).  All lanes of
+// the warp must call.
+template <int TPA>
+__device__ __forceinline__ void combine_lanes(double &Fx, double &Fy, double &Fz) {
+#pragma unroll
+  for (int o = 1; o < TPA; o <<= 1) {
+    Fx = Fx + __shfl_xor_sync(0xffffffffu, Fx, o);
+    Fy = Fy + __shfl_xor_sync(0xffffffffu, Fy, o);
+    Fz = Fz + __shfl_xor_sync(0xffffffffu, Fz, o);
+  }
+}
+
+// FP32-mixed force kick, TPA lanes per atom.  Displacements come from the
+// fixed-point copy (no ghost atoms, no shift codes); the row sum is
+// fp32_row_part's fixed-order tree and the kick is FP64 (lane 0 of the
+// atom).  With DRIFT the second half drift q += v dt/2 and the |v| maximum
+// of the step are done in the same pass: this kernel reads only the
 // fixed-point copy, so moving q here races with no other thread.  DRIFT == 2
 // is the whole NVE step in one pass: qf holds every atom's position after
 // this step's first half drift (packed by the previous step's pass, or by
@@ -1374,23 +1640,27 @@ __device__ __forceinline__ void fp32_row_staged(const Arrays &a, const Box &b, c
 // into qf_next (the other buffer, so no thread overwrites a copy that
 // another still reads).  The arithmetic is the separate drift kernels',
 // operation for operation.
-template <int BLOCK, int MODE, int DRIFT>
+template <int BLOCK, int MODE, int DRIFT, int TPA>
 __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Thermo th, const int4 *qf,
                                                       int4 *qf_next) {
-  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  const int t = blockIdx.x * BLOCK + threadIdx.x;
+  const int i = t / TPA, sub = t % TPA;
   double v2 = 0.0, ke = 0.0;
-  if (DRIFT == 2 && MODE == kKick && i == 0 && !a.st->error) {
+  if (DRIFT == 2 && MODE == kKick && t == 0 && !a.st->error) {
     // the step counter (k_step_done's work): nothing in this pass reads it
     a.st->steps++;
     a.st->sim_time += b.dt;
   }
-  if (i < n && !a.st->error) {
-    const int4 pi = qf[i];
-    const int nn4 = (a.nnbr[i] + 3) & ~3;
-    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-    fp32_row_global(a, b, qf, i, pi, nn4, Fx, Fy, Fz);
-    fp32_finish<MODE, DRIFT>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
+  const bool active = i < n && !a.st->error;
+  double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+  int4 pi = make_int4(0, 0, 0, 0);
+  if (active) {
+    pi = qf[i];
+    GlobalGroups f{a.nbr + i, a.stride, qf, i};
+    fp32_row_part<TPA>(f, (a.nnbr[i] + 3) >> 2, sub, pi, pair_const(b.fix_scale, b.rc2f, b.c2x8f), Fx, Fy, Fz);
   }
+  combine_lanes<TPA>(Fx, Fy, Fz);
+  if (active && sub == 0) fp32_finish<MODE, DRIFT>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
   if (MODE == kKickLangevin || DRIFT) warp_max_to(&a.st->vmax2_bits, v2);
   if (MODE == kKickNoseHoover) {
     double s[1] = {ke};
@@ -1510,16 +1780,140 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32_staged(Arrays a, Box b, in
   }
   if (ok && i < n && !a.st->error) {
     const int4 pi = qf[i];
-    const int nn4 = (a.nnbr[i] + 3) & ~3;
+    const int G = (a.nnbr[i] + 3) >> 2;
+    const PairConst k = pair_const(b.fix_scale, b.rc2f, b.c2x8f);
     double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-    if (use_stage) fp32_row_staged(a, b, pos, nstage, i, pi, nn4, Fx, Fy, Fz);
-    else fp32_row_global(a, b, qf, i, pi, nn4, Fx, Fy, Fz);
+    if (use_stage) {
+      StagedGroups f{a.nbr16 + i, a.stride, pos, nstage};
+      fp32_row_part<1>(f, G, 0, pi, k, Fx, Fy, Fz);
+      if (f.bad) atomicOr(&a.st->error, kErrStage);
+    } else {
+      GlobalGroups f{a.nbr + i, a.stride, qf, i};
+      fp32_row_part<1>(f, G, 0, pi, k, Fx, Fy, Fz);
+    }
     fp32_finish<MODE, DRIFT>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
   }
   if (MODE == kKickLangevin || DRIFT) warp_max_to(&a.st->vmax2_bits, v2);
   if (MODE == kKickNoseHoover) {
     double s[1] = {ke};
     block_sum_to<BLOCK, 1>(s, a.partials);
+  }
+}
+
+// ------------------------------------------- persistent multi-step NVE pass
+// Grid barrier for a cooperative launch (every block resident): a counter
+// and a generation number.  A block waits at most `limit` polls; one that
+// gives up sets kErrTimeout and returns false, and the caller leaves its
+// loop (so does every other block at its next barrier).
+struct GridBarrier {
+  unsigned count;
+  unsigned gen;
+};
+
+__device__ __forceinline__ bool grid_barrier(GridBarrier *g, Status *st, long long limit) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    const unsigned gen = *(volatile unsigned *)&g->gen;
+    __threadfence();
+    if (atomicAdd(&g->count, 1u) + 1u == gridDim.x) {
+      g->count = 0u;
+      __threadfence();
+      atomicAdd(&g->gen, 1u);
+    } else {
+      long long polls = 0;
+      while (*(volatile unsigned *)&g->gen == gen) {
+        if (++polls > limit) {
+          atomicOr(&st->error, kErrTimeout);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// About a second of polling at 64 ns per poll: a step takes microseconds.
+constexpr long long kBarrierPolls = 16000000ll;
+
+// The expiry test of PairList::IsPairListExpired (k_expiry's arithmetic)
+// for a step the persistent pass may take on its own: the list is current,
+// the skin budget is positive and stays non-negative after this step's
+// 2 vmax dt.  Only then is the budget spent and the |v| maximum cleared;
+// otherwise nothing changes and the caller's ordinary step (k_expiry, the
+// displacement check, the rebuild) takes this step.
+__device__ __forceinline__ bool take_step_alone(Status *st, const Box &b) {
+  if (st->error || st->list_stale || !(st->budget > 0.0)) return false;
+  const double vmax = sqrt(__longlong_as_double((long long)st->vmax2_bits));
+  if (vmax * 2.0 * b.dt > b.buffer_length) return false;  // k_expiry reports the too-fast atom
+  const double budget = st->budget - vmax * 2.0 * b.dt;
+  if (budget < 0.0) return false;
+  st->budget = budget;
+  st->vmax2_bits = 0ull;
+  return true;
+}
+
+// Up to max_steps FP32-mixed NVE steps in one cooperative launch, for
+// systems small enough that per-step launch latency dominates: each step is
+// the fused pass of k_force_fp32<.., kKick, 2, TPA> over all atoms
+// (grid-stride), between two grid barriers -- one after the pass (every
+// position packed, the |v| maximum complete), one after block 0 has taken
+// the expiry decision.  The pass stops before the first step that needs the
+// displacement check or a rebuild, and before any error; out[0] returns the
+// steps taken, out[1] which fixed-point buffer holds the next step's
+// first-drift positions (0: qf0, 1: qf1).  The arithmetic is
+// k_force_fp32's, so trajectories equal the graph path's bit for bit.
+template <int BLOCK, int TPA>
+__global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n, int max_steps, int4 *qf0,
+                                                          int4 *qf1, int parity, GridBarrier *bar, int *out) {
+  __shared__ int go;
+  const Thermo th{};
+  const PairConst k = pair_const(b.fix_scale, b.rc2f, b.c2x8f);
+  const long long nthreads = (long long)n * TPA;
+  const long long stride = (long long)gridDim.x * BLOCK;
+  int steps = 0;
+  for (; steps < max_steps; steps++) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      const int g = take_step_alone(a.st, b) ? 1 : 0;
+      *(volatile int *)&out[2] = g;
+      if (g) {
+        a.st->steps++;
+        a.st->sim_time += b.dt;
+      }
+      __threadfence();
+    }
+    if (!grid_barrier(bar, a.st, kBarrierPolls)) break;
+    if (threadIdx.x == 0) go = *(volatile int *)&out[2];
+    __syncthreads();
+    if (!go) break;
+    const int4 *qf = parity ? qf1 : qf0;
+    int4 *qf_next = parity ? qf0 : qf1;
+    // warps walk whole warps of threads, so the lane shuffles stay converged
+    for (long long base = (long long)blockIdx.x * BLOCK + (threadIdx.x & ~31); base < nthreads; base += stride) {
+      const long long t = base + (threadIdx.x & 31);
+      const int i = (int)(t / TPA), sub = (int)(t % TPA);
+      const bool active = t < nthreads && !a.st->error;
+      double Fx = 0.0, Fy = 0.0, Fz = 0.0, v2 = 0.0, ke = 0.0;
+      if (active) {
+        const int4 pi = qf[i];
+        GlobalGroups f{a.nbr + i, a.stride, qf, i};
+        fp32_row_part<TPA>(f, (a.nnbr[i] + 3) >> 2, sub, pi, k, Fx, Fy, Fz);
+      }
+      combine_lanes<TPA>(Fx, Fy, Fz);
+      if (active && sub == 0) fp32_finish<kKick, 2>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
+      warp_max_to(&a.st->vmax2_bits, v2);
+    }
+    parity ^= 1;
+    if (!grid_barrier(bar, a.st, kBarrierPolls)) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    out[0] = steps;
+    out[1] = parity;
   }
 }
 

@@ -38,6 +38,7 @@ struct Rep {
   float fix_scale[3];
   int ms[3];
   int ncell, cell_off, atom_off, n;
+  long long tab_off;  // first entry of the replica's rows in the trim table
   int small;  // all-pairs search (fewer than 3 cells along an axis)
 };
 
@@ -70,6 +71,7 @@ struct Ens {
   double4 *q, *v, *q_old;
   int4 *qfix;
   float4 *qloc;
+  int *cxyz, *xsub;  // packed cell coordinates and the list-build trim table (as the single-system arrays)
   int *ids, *cell, *cell_tmp, *nbr, *nnbr, *cell_count, *cell_start, *slot, *perm, *perm2;
   double lag;  // age of the reference's ghost copies at the skin check
   double4 *q_tmp, *v_tmp;
@@ -108,6 +110,9 @@ __device__ __forceinline__ Box box_of(const Ens &e, const Rep &r) {
   b.check_list_length = e.cll;
   b.sl2_lo = e.sl2_lo;
   b.sl2_hi = e.sl2_hi;
+  b.slab = 0;
+  b.z0 = 0;
+  b.nzl = r.ms[2];
   return b;
 }
 
@@ -427,28 +432,13 @@ __global__ void __launch_bounds__(kEB) ke_scatter(Ens e) {
 }
 
 // Warp per cell of a rebuilding replica (the cells of the rebuild work
-// list): order by upload id.
-__device__ __forceinline__ void sort_cell(const Ens &e, int cell, int lane) {
+// list): order by (x, upload id) and the cell's row of the trim table, as
+// the single-system k_sort_cells.
+__device__ __forceinline__ void sort_cell(const Ens &e, const Rep &rep, int cell, int lane) {
   const int beg = e.cell_start[cell], cnt = e.cell_start[cell + 1] - beg;
-  for (int base = 0; base < cnt; base += 32) {
-    const int me = base + lane;
-    int my_slot = -1, my_key = 0x7fffffff;
-    if (me < cnt) {
-      my_slot = e.perm[beg + me];
-      my_key = e.ids[my_slot];
-    }
-    int rank = 0;
-    for (int ob = 0; ob < cnt; ob += 32) {
-      const int other = ob + lane;
-      int okey = 0x7fffffff;
-      if (other < cnt) okey = e.ids[e.perm[beg + other]];
-      for (int k = 0; k < 32; k++) {
-        const int kk = __shfl_sync(0xffffffffu, okey, k);
-        if (ob + k < cnt && kk < my_key) rank++;
-      }
-    }
-    if (me < cnt) e.perm2[beg + rank] = my_slot;
-  }
+  const int c = cell - rep.cell_off, cx = c % rep.ms[0];
+  sort_cell_x(e.q, e.ids, e.perm, e.perm2, beg, cnt, cx * rep.cs[0], rep.cs[0] / kXSub,
+              trim_entries(e.xsub + rep.tab_off, rep.ms[0], c / rep.ms[0], cx), cx == rep.ms[0] - 1, lane);
 }
 
 __global__ void __launch_bounds__(kEB) ke_sort_cells(Ens e) {
@@ -458,7 +448,8 @@ __global__ void __launch_bounds__(kEB) ke_sort_cells(Ens e) {
   const int wstride = gridDim.x * (kEB / 32);
   for (int gc = blockIdx.x * (kEB / 32) + (threadIdx.x >> 5); gc < total; gc += wstride) {
     const int k = work_find(e.wb.cell_prefix, nk, gc);
-    sort_cell(e, e.rep[e.wb.rep[k]].cell_off + (gc - e.wb.cell_prefix[k]), lane);
+    const Rep &rep = e.rep[e.wb.rep[k]];
+    sort_cell(e, rep, rep.cell_off + (gc - e.wb.cell_prefix[k]), lane);
   }
 }
 
@@ -481,8 +472,8 @@ __device__ __forceinline__ int permute_atom(const Ens &e, int r, int s) {
   e.mult[s] = (unsigned char)border_bits(x, b, &m);
   const int c = cg - rep.cell_off;
   const int cx = c % rep.ms[0], cy = (c / rep.ms[0]) % rep.ms[1], cz = c / (rep.ms[0] * rep.ms[1]);
-  e.qloc[s] = make_float4((float)(q.x - cx * rep.cs[0]), (float)(q.y - cy * rep.cs[1]),
-                          (float)(q.z - cz * rep.cs[2]), 0.f);
+  e.qloc[s] = make_float4((float)q.x, (float)(q.y - cy * rep.cs[1]), (float)(q.z - cz * rep.cs[2]), 0.f);
+  e.cxyz[s] = pack_cell(cx, cy, cz);
   return m;
 }
 
@@ -514,9 +505,8 @@ __global__ void __launch_bounds__(kEB) ke_copy_back(Ens e) {
 }
 
 // One atom's row of the list build, as the single-system build makes it
-// (same candidate order, same FP32 prefilter with the exact FP64 band);
-// all-pairs with the minimum image for small replicas.  Returns the entries
-// kept.
+// (build_rows: same rows in the same order); all-pairs with the minimum
+// image for small replicas.  Returns the entries kept.
 __device__ __forceinline__ int ens_build_row(const Ens &e, int i) {
   const int r = e.rep_of[i];
   RepStatus &st = e.rs[r];
@@ -540,52 +530,10 @@ __device__ __forceinline__ int ens_build_row(const Ens &e, int i) {
       cnt++;
     }
   } else {
-    const float4 li = e.qloc[i];
-    const int c = e.cell_tmp[i] - rep.cell_off;
-    const int cx = c % rep.ms[0], cy = (c / rep.ms[0]) % rep.ms[1], cz = c / (rep.ms[0] * rep.ms[1]);
-    const float lo = e.sl2_lo, hi = e.sl2_hi;
-    for (int dz = -1; dz <= 1; dz++) {
-      int z = cz + dz;
-      double sz = 0.0;
-      if (z < 0) { z += rep.ms[2]; sz = -rep.L[2]; } else if (z >= rep.ms[2]) { z -= rep.ms[2]; sz = rep.L[2]; }
-      const float bz = (float)((z - cz) * rep.cs[2] + sz) - li.z;
-      for (int dy = -1; dy <= 1; dy++) {
-        int y = cy + dy;
-        double sy = 0.0;
-        if (y < 0) { y += rep.ms[1]; sy = -rep.L[1]; } else if (y >= rep.ms[1]) { y -= rep.ms[1]; sy = rep.L[1]; }
-        const float by = (float)((y - cy) * rep.cs[1] + sy) - li.y;
-        for (int dx = -1; dx <= 1; dx++) {
-          int x = cx + dx;
-          double sx = 0.0;
-          if (x < 0) { x += rep.ms[0]; sx = -rep.L[0]; } else if (x >= rep.ms[0]) { x -= rep.ms[0]; sx = rep.L[0]; }
-          const float bx = (float)((x - cx) * rep.cs[0] + sx) - li.x;
-          const int nc = rep.cell_off + (z * rep.ms[1] + y) * rep.ms[0] + x;
-          const int beg = e.cell_start[nc], end = e.cell_start[nc + 1];
-          const int need = needed_strips(sx, sy, sz);
-          // one candidate, in row order (as the single-system build)
-          auto accept = [&](int j, float r2) {
-            if (r2 > hi || j == i) return;
-            if (need && (e.mult[j] & need) != need) return;
-            if (r2 >= lo && !within_search_exact(e.q[i], e.q[j], sx, sy, sz, e.sl2)) return;
-            if (cnt < maxnb) e.nbr[(size_t)cnt * stride + i] = j;
-            cnt++;
-          };
-          auto dist2f = [&](const float4 &lj) {
-            const float ex = lj.x + bx, ey = lj.y + by, ez = lj.z + bz;
-            return fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-          };
-          // two candidates per iteration, both loads issued first
-          int j = beg;
-          for (; j + 1 < end; j += 2) {
-            const float4 l0 = e.qloc[j], l1 = e.qloc[j + 1];
-            const float r0 = dist2f(l0), r1 = dist2f(l1);
-            accept(j, r0);
-            accept(j + 1, r1);
-          }
-          if (j < end) accept(j, dist2f(e.qloc[j]));
-        }
-      }
-    }
+    auto emit = [&](int j, int k) {
+      if (k < maxnb) e.nbr[(size_t)k * stride + i] = j;
+    };
+    cnt = build_rows(box_of(e, rep), e.qloc, e.q, e.mult, e.xsub + rep.tab_off, e.cxyz[i], i, emit);
   }
   e.nnbr[i] = min(cnt, maxnb);
   if (cnt > maxnb) {
@@ -648,68 +596,23 @@ __global__ void __launch_bounds__(kEB) ke_drift(Ens e, int track_vmax) {
 
 // FP32-mixed kick with the second half drift fused (the single-system
 // k_force_fp32 loop on the replica's fixed-point scale).
+template <int TPA>
 __global__ void __launch_bounds__(kEF) ke_force_fp32(Ens e) {
-  const int i = blockIdx.x * kEF + threadIdx.x;
+  const int t = blockIdx.x * kEF + threadIdx.x;
+  const int i = t / TPA, sub = t % TPA;
   int r = 0;
   double v2 = 0.0;
   const bool active = i < e.ntot && !*e.error;
+  double Fx = 0.0, Fy = 0.0, Fz = 0.0;
   if (active) {
     r = e.rep_of[i];
     const Rep &rep = e.rep[r];
-    const int4 pi = e.qfix[i];
-    const int nn4 = (e.nnbr[i] + 3) & ~3;
-    const float sx = rep.fix_scale[0], sy = rep.fix_scale[1], sz = rep.fix_scale[2];
-    const unsigned rc2_bits = __float_as_uint(e.rc2f);
-    const float c2x8 = e.c2x8f;
-    const int *row = e.nbr + i;
-    const int st = e.stride;
-    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-    float fx = 0.f, fy = 0.f, fz = 0.f;
-    // indices of the next eight partners in flight, as in k_force_fp32
-    int n0 = i, n1 = i, n2 = i, n3 = i;
-    int m0 = i, m1 = i, m2 = i, m3 = i;
-    if (nn4 > 0) {
-      n0 = __ldg(row);
-      n1 = __ldg(row + st);
-      n2 = __ldg(row + 2 * st);
-      n3 = __ldg(row + 3 * st);
-    }
-    if (nn4 > 4) {
-      m0 = __ldg(row + 4 * st);
-      m1 = __ldg(row + 5 * st);
-      m2 = __ldg(row + 6 * st);
-      m3 = __ldg(row + 7 * st);
-    }
-    for (int k = 0; k < nn4; k += 4) {
-      const int4 p0 = __ldg(e.qfix + n0);
-      const int4 p1 = __ldg(e.qfix + n1);
-      const int4 p2 = __ldg(e.qfix + n2);
-      const int4 p3 = __ldg(e.qfix + n3);
-      n0 = m0;
-      n1 = m1;
-      n2 = m2;
-      n3 = m3;
-      if (k + 8 < nn4) {
-        const int *rr = row + (size_t)(k + 8) * st;
-        m0 = __ldg(rr);
-        m1 = __ldg(rr + st);
-        m2 = __ldg(rr + 2 * st);
-        m3 = __ldg(rr + 3 * st);
-      }
-      lj_pair_fp32(pi, p0, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-      lj_pair_fp32(pi, p1, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-      lj_pair_fp32(pi, p2, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-      lj_pair_fp32(pi, p3, sx, sy, sz, rc2_bits, c2x8, fx, fy, fz);
-      if (k & 4) {
-        Fx += (double)fx;
-        Fy += (double)fy;
-        Fz += (double)fz;
-        fx = fy = fz = 0.f;
-      }
-    }
-    Fx += (double)fx;
-    Fy += (double)fy;
-    Fz += (double)fz;
+    GlobalGroups f{e.nbr + i, e.stride, e.qfix, i};
+    fp32_row_part<TPA>(f, (e.nnbr[i] + 3) >> 2, sub, e.qfix[i], pair_const(rep.fix_scale, e.rc2f, e.c2x8f), Fx, Fy,
+                       Fz);
+  }
+  combine_lanes<TPA>(Fx, Fy, Fz);
+  if (active && sub == 0) {
     const double dt = e.dt;
     double4 v = e.v[i];
     v.x = dadd(v.x, Fx * dt);
@@ -725,7 +628,7 @@ __global__ void __launch_bounds__(kEF) ke_force_fp32(Ens e) {
     v2 = dadd(dadd(dmul(v.x, v.x), dmul(v.y, v.y)), dmul(v.z, v.z));
     if (!isfinite(v2) || !isfinite(q.x + q.y + q.z)) atomicOr(e.error, kErrNonFinite);
   }
-  rep_max(&e.rs[0].vmax2_bits, sizeof(RepStatus), r, v2, active);
+  rep_max(&e.rs[0].vmax2_bits, sizeof(RepStatus), r, v2, active);  // v2 = 0 on lanes other than 0
 }
 
 // FP64 kick (the single-system k_force_fp64 pair terms).
@@ -861,6 +764,12 @@ struct mdg_ensemble {
   std::vector<cudaEvent_t> ev;  // 2 per captured step
   double force_ms = 0.0;
   int64_t force_launches = 0;
+  // lanes per atom of the FP32 force pass: chosen (1, 2, 4) or 0 while the
+  // first steps time each candidate (tune_lanes is the one the next eager
+  // step uses); the forces are bit-identical for every choice
+  int tpa = 0;
+  int tune_lanes = 1;
+  float tune_ms[3] = {0.f, 0.f, 0.f};
 };
 
 namespace {
@@ -877,7 +786,7 @@ cudaError_t edalloc(T **p, size_t count) {
 
 void e_free(mdg_ensemble *x) {
   Ens &e = x->e;
-  void *ptrs[] = {(void *)e.rep, e.rs, (void *)e.rep_of, e.q, e.v, e.q_old, e.qfix, e.qloc, e.ids, e.cell,
+  void *ptrs[] = {(void *)e.rep, e.rs, (void *)e.rep_of, e.q, e.v, e.q_old, e.qfix, e.qloc, e.cxyz, e.xsub, e.ids, e.cell,
                   e.cell_tmp, e.nbr, e.nnbr, e.cell_count, e.cell_start, e.slot, e.perm, e.perm2, e.q_tmp,
                   e.v_tmp, e.ids_tmp, e.mult, e.cand, e.error, e.sums, x->d_flags, x->d_count,
                   x->d_lists};
@@ -932,7 +841,11 @@ int e_launch_tail(mdg_ensemble *x, cudaStream_t s, cudaEvent_t e0 = nullptr, cud
   if (x->prm.precision == MDG_FP32_MIXED) {
     ke_drift<true><<<nb(e.ntot, kEB), kEB, 0, s>>>(e, 0);
     rec(e0);
-    ke_force_fp32<<<nb(e.ntot, kEF), kEF, 0, s>>>(e);
+    const int lanes = x->tpa > 0 ? x->tpa : x->tune_lanes;
+    const int blocks = (int)(((long long)e.ntot * lanes + kEF - 1) / kEF);
+    if (lanes == 4) ke_force_fp32<4><<<blocks, kEF, 0, s>>>(e);
+    else if (lanes == 2) ke_force_fp32<2><<<blocks, kEF, 0, s>>>(e);
+    else ke_force_fp32<1><<<blocks, kEF, 0, s>>>(e);
     rec(e1);
     ke_step_done<<<1, 1024, 0, s>>>(e);
     return 3;
@@ -1040,7 +953,7 @@ mdg_status e_build_graph(mdg_ensemble *x) {
   return MDG_OK;
 }
 
-mdg_status e_step_eager(mdg_ensemble *x) {
+mdg_status e_step_eager(mdg_ensemble *x, float *force_ms_out = nullptr) {
   int flags[2] = {0, 0};
   ke_expiry<<<1, 1024, 0, x->stream>>>(x->e, 0, 0, x->d_flags);
   ECUDA(cudaMemcpyAsync(flags, x->d_flags, sizeof flags, cudaMemcpyDeviceToHost, x->stream));
@@ -1053,21 +966,25 @@ mdg_status e_step_eager(mdg_ensemble *x) {
   x->kernel_launches++;
   if (flags[1]) e_launch_build(x, x->stream);  // counted on the device (ke_decide)
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (x->timing) {
+  const bool timed = x->timing || force_ms_out;
+  if (timed) {
     ECUDA(cudaEventCreate(&e0));
     ECUDA(cudaEventCreate(&e1));
   }
   x->kernel_launches += e_launch_tail(x, x->stream, e0, e1);
   ECUDA(cudaGetLastError());
-  if (x->timing) {
+  if (timed) {
     float ms = 0.f;
     cudaError_t err = cudaEventSynchronize(e1);
     if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ECUDA(err);
-    x->force_ms += ms;
-    x->force_launches++;
+    if (x->timing) {
+      x->force_ms += ms;
+      x->force_launches++;
+    }
+    if (force_ms_out) *force_ms_out = ms;
   }
   return MDG_OK;
 }
@@ -1141,8 +1058,14 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
   const double SL = prm->cutoff + prm->buffer_length;
   mdg_ensemble *x = new mdg_ensemble();
   x->prm = *prm;
+  if (prm->threads_per_atom != 0 && prm->threads_per_atom != 1 && prm->threads_per_atom != 2 &&
+      prm->threads_per_atom != 4) {
+    delete x;
+    return MDG_ERR_INVALID_ARGUMENT;
+  }
+  x->tpa = prm->threads_per_atom;
   x->reps.resize(nrep);
-  long long atoms = 0;
+  long long atoms = 0, tab_entries = 0;
   int cells = 0;
   for (int r = 0; r < nrep; r++) {
     Rep &rp = x->reps[r];
@@ -1171,8 +1094,14 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
       rp.cs[d] = rp.L[d] / (double)rp.ms[d];
     }
     rp.small = small;
+    if (rp.ms[0] >= 2048 || rp.ms[1] >= 2048 || rp.ms[2] >= 1024) {  // packed cell coordinates (pack_cell)
+      delete x;
+      return MDG_ERR_INVALID_ARGUMENT;
+    }
     rp.ncell = rp.ms[0] * rp.ms[1] * rp.ms[2];
     rp.cell_off = cells;
+    rp.tab_off = tab_entries;
+    tab_entries += (long long)rp.ms[1] * rp.ms[2] * (rp.ms[0] * kXSub + 1);
     rp.atom_off = (int)atoms;
     rp.n = replicas[r].n;
     cells += rp.ncell;
@@ -1201,8 +1130,11 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
   e.lag = 0.5 * prm->time_step;  // NVE: ghosts refreshed before the last half drift
   e.rc2f = (float)e.rc2;
   e.c2x8f = (float)(e.c2 * 8.0);
-  e.sl2_lo = (float)(e.sl2 * (1.0 - 1e-4));
-  e.sl2_hi = (float)(e.sl2 * (1.0 + 1e-4));
+  {
+    double lx = 0.0;
+    for (int r = 0; r < nrep; r++) lx = std::max(lx, x->reps[r].L[0]);
+    prefilter_band(e.sl2, SL, lx, &e.sl2_lo, &e.sl2_hi);
+  }
   x->ncell_tot = cells;
   const size_t n = (size_t)std::max<long long>(atoms, 1);
   cudaError_t err = cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking);
@@ -1219,6 +1151,8 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
   if (err == cudaSuccess) err = edalloc(&e.q_old, n);
   if (err == cudaSuccess) err = edalloc(&e.qfix, n);
   if (err == cudaSuccess) err = edalloc(&e.qloc, n);
+  if (err == cudaSuccess) err = edalloc(&e.cxyz, n);
+  if (err == cudaSuccess) err = edalloc(&e.xsub, (size_t)tab_entries);
   if (err == cudaSuccess) err = edalloc(&e.ids, n);
   if (err == cudaSuccess) err = edalloc(&e.cell, n);
   if (err == cudaSuccess) err = edalloc(&e.cell_tmp, n);
@@ -1361,6 +1295,23 @@ mdg_status mdg_ensemble_calculate(mdg_ensemble *x, int nsteps) {
   for (int attempt = 0; attempt < 8; attempt++) {
     long long left = target - rs[0].steps;
     if (left <= 0) break;
+    // FP32-mixed with the lanes per atom to be chosen: the first steps run
+    // one candidate each (1, 2, 4 lanes) with the force pass timed; the
+    // steps are the trajectory's own (every choice gives the same forces)
+    while (x->prm.precision == MDG_FP32_MIXED && x->tpa == 0 && left > 0) {
+      const int k = x->tune_lanes == 1 ? 0 : (x->tune_lanes == 2 ? 1 : 2);
+      if ((r = e_step_eager(x, &x->tune_ms[k]))) return r;
+      left--;
+      if (k < 2) {
+        x->tune_lanes *= 2;
+      } else {
+        int best = 0;
+        for (int c = 1; c < 3; c++)
+          if (x->tune_ms[c] < x->tune_ms[best]) best = c;
+        x->tpa = 1 << best;
+        x->graph_dirty = true;
+      }
+    }
     if (x->use_graphs && left >= kEStepsPerGraph && x->graph_dirty) {
       if ((r = e_build_graph(x))) return r;
     }
@@ -1505,3 +1456,33 @@ mdg_status mdg_ensemble_kernel_time(mdg_ensemble *x, double *force_ms, int64_t *
 void *mdg_ensemble_stream(mdg_ensemble *x) { return x ? (void *)x->stream : nullptr; }
 
 }  // extern "C"
+
+// ------------------------------------------------------- replica partition
+extern "C" mdg_status mdg_partition_replicas(const mdg_replica *replicas, int nrep, double search_length,
+                                             int nranks, int *owner, double *load) {
+  if (nrep < 0 || nranks < 1 || !(search_length > 0.0) || (nrep > 0 && (!replicas || !owner)))
+    return MDG_ERR_INVALID_ARGUMENT;
+  std::vector<double> cost(nrep);
+  const double sphere = 4.0 / 3.0 * M_PI * search_length * search_length * search_length;
+  for (int r = 0; r < nrep; r++) {
+    const mdg_replica &x = replicas[r];
+    if (x.n < 0 || !(x.L[0] > 0.0) || !(x.L[1] > 0.0) || !(x.L[2] > 0.0)) return MDG_ERR_INVALID_ARGUMENT;
+    const double rho = (double)x.n / (x.L[0] * x.L[1] * x.L[2]);
+    cost[r] = (double)x.n * (41.0 + sphere * rho);
+  }
+  std::vector<int> order(nrep);
+  for (int r = 0; r < nrep; r++) order[r] = r;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::vector<double> tot(nranks, 0.0);
+  for (int r : order) {
+    int best = 0;
+    for (int k = 1; k < nranks; k++)
+      if (tot[k] < tot[best]) best = k;
+    owner[r] = best;
+    tot[best] += cost[r];
+  }
+  if (load)
+    for (int k = 0; k < nranks; k++) load[k] = tot[k];
+  return MDG_OK;
+}
+

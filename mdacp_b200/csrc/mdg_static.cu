@@ -14,12 +14,20 @@
 // 8192 blocks of 256 atoms, 2,097,152 atoms; larger inputs are refused with
 // MDG_ERR_CAPACITY.
 //
-// The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress, once per device, with that device current); make
-// that first call before any stream capture.  Every call on a device shares
-// the array and leaves its partial sums in it; each call writes every slot
-// it later reads, so nothing needs clearing, but calls whose kernels overlap
-// on the GPU (different streams, no ordering between them) race on it.
+// The array's device address comes from cudaGetSymbolAddress with the
+// call's device current.  A call on a stream that is not being captured
+// looks it up again every time (cheap once the module is loaded), so a
+// cudaDeviceReset, after which the module may load the array elsewhere, is
+// harmless; a call made during a stream capture uses the address the last
+// uncaptured call on that device found, so make one call on each device
+// before capturing any.  Every call on a device shares the array and leaves
+// its partial sums in it; each call writes every slot it later reads, so
+// nothing needs clearing, but calls whose kernels overlap on the GPU
+// (different streams, no ordering between them) race on it.
+//
+// The partner indices are the caller's: an index outside [0, n) is skipped
+// (never read) and turns the result's potential energy into NaN, so a bad
+// list shows up in the output rather than as a device fault.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -79,7 +87,12 @@ __global__ void __launch_bounds__(kStaticBlock)
     ke = sadd(sadd(smul(smul(0.5, vi.x), vi.x), smul(smul(0.5, vi.y), vi.y)), smul(smul(0.5, vi.z), vi.z));
     const double4 qi = q[i];
     for (int k = row_start[i]; k < row_start[i + 1]; k++) {
-      const double4 qj = q[partners[k]];
+      const int j = partners[k];
+      if ((unsigned)j >= (unsigned)n) {  // not an atom of this call: skipped, reported as NaN
+        pe = __longlong_as_double(0x7ff8000000000000ll);
+        continue;
+      }
+      const double4 qj = q[j];
       const double dx = ssub(qi.x, simage(qj.x, qi.x, b.L[0], b.hL[0]));
       const double dy = ssub(qi.y, simage(qj.y, qi.y, b.L[1], b.hL[1]));
       const double dz = ssub(qi.z, simage(qj.z, qi.z, b.L[2], b.hL[2]));
@@ -130,20 +143,25 @@ __global__ void __launch_bounds__(kStaticBlock) k_observe_static_final(const dou
   }
 }
 
-// Device address of the scratch array on the current device, looked up once
-// per device (cudaGetSymbolAddress) with that device current.
-mdg_status scratch_for_current_device(double **out) {
+// Device address of the scratch array on the current device, with that
+// device current.  Outside a stream capture it is looked up on every call
+// (and kept); during a capture the kept value of the device is used.
+mdg_status scratch_for_current_device(cudaStream_t s, double **out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return MDG_ERR_NO_DEVICE;
   if (dev < 0 || dev >= kStaticMaxDevices) return MDG_ERR_INVALID_ARGUMENT;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(s, &cs);
+  if (e != cudaSuccess) return MDG_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
+  if (cs == cudaStreamCaptureStatusNone) {
     void *addr = nullptr;
     e = cudaGetSymbolAddress(&addr, g_observe_scratch);
-    if (e != cudaSuccess || !addr)
-      return MDG_ERR_CUDA;
+    if (e != cudaSuccess || !addr) return MDG_ERR_CUDA;
     g_scratch_addr[dev] = static_cast<double *>(addr);
+  } else if (!g_scratch_addr[dev]) {
+    return MDG_ERR_STATE;  // no uncaptured call on this device yet
   }
   *out = g_scratch_addr[dev];
   return MDG_OK;
@@ -175,10 +193,13 @@ extern "C" mdg_status mdg_observe_static(const double *q4, const double *v4, int
   const double s6 = s2 * s2 * s2, s8 = s6 * s2, s12 = s6 * s6, s14 = s12 * s2;
   b.c2 = 6.0 * s14 - 3.0 * s8;
   b.c0 = -s12 + s6 - b.c2 / s2;
-  double *scratch = nullptr;
-  mdg_status r = mdg::scratch_for_current_device(&scratch);
-  if (r) return r;
+  // an error the caller's own earlier work left pending is theirs: report
+  // it without clearing it and launch nothing
+  if (cudaPeekAtLastError() != cudaSuccess) return MDG_ERR_CUDA;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double *scratch = nullptr;
+  mdg_status r = mdg::scratch_for_current_device(s, &scratch);
+  if (r) return r;
   const int nblocks = n > 0 ? (n + kStaticBlock - 1) / kStaticBlock : 1;
   mdg::k_observe_csr_static<<<nblocks, kStaticBlock, 0, s>>>(reinterpret_cast<const double4 *>(q4),
                                                         reinterpret_cast<const double4 *>(v4), n, row_start,

@@ -8,12 +8,12 @@
 # the GPU through libmdacp_b200.so.  CUTOFF_LENGTH is the reference's
 # compile-time constant (include/mdconfig.h:31); one binary per cut-off:
 #   mdacp_b200/dropin/_build/mdacp_rc25   mdacp_b200/dropin/_build/mdacp_rc30
-# Usage: mdacp_b200/dropin/build_dropin.sh [REFERENCE_ROOT]
+# Usage: mdacp_b200/dropin/build_dropin.sh REFERENCE_ROOT   (or MDACP_REFERENCE=REFERENCE_ROOT)
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 PKG="$(cd "$HERE/.." && pwd)"
 REPO="$(cd "$PKG/.." && pwd)"
-REF="${1:-${MDACP_REFERENCE:-/root/reference}}"
+REF="${1:-${MDACP_REFERENCE:-}}"
 OUT="$HERE/_build"
 if [ ! -f "$REF/src/main.cc" ]; then
   echo "build_dropin: reference sources not found at $REF" >&2

@@ -7,6 +7,9 @@
 //   Precision=FP64|FP32Mixed   (default FP64, the drop-in arithmetic)
 //   Capacity=<atoms>           (default mdconfig.h N)
 //   Device=<cuda ordinal>      (default 0)
+//   DeviceExecutors=yes|no     (default yes) an executor the drop-in knows
+//                              runs on the device after every step instead of
+//                              on the host mirror (see ExecuteAll)
 #ifndef mdmanager_h
 #define mdmanager_h
 #include <vector>
@@ -30,6 +33,9 @@ class MDManager {
   double s_time;
   bool control_synced;
   void SyncControl(void);
+  bool device_executors;
+  Executor *routed;  // the executor running on the device, if any
+  bool RouteToDevice(Executor *ex);
 
  public:
   MDManager(int &argc, char **&argv);

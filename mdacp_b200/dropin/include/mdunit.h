@@ -37,6 +37,7 @@ class MDUnit {
   MDRect myrect;
   mdg_handle *dev;
   int precision;
+  Variables *probe;  // while set, GetVariables hands out this scratch set (ProbeUniformKick)
   void CreateDevice(void);
 
  public:
@@ -81,5 +82,9 @@ class MDUnit {
   mdg_handle *Device(void) { return dev; }
   Variables *Vars(void) { return vars; }
   void SetControl(void);
+  // Runs ex once on two scratch atoms (different positions and momenta)
+  // instead of the unit's own: true, with the change of p in dp, if ex
+  // added the same dp to both and moved neither -- a uniform kick.
+  bool ProbeUniformKick(Executor *ex, double dp[D]);
 };
 #endif

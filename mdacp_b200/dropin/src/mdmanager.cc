@@ -5,16 +5,21 @@
 
 #include <mpi.h>
 
+#include <cxxabi.h>
+
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <fstream>
+#include <string>
+#include <typeinfo>
 
 #include "cmdline.h"
 #include "communicator.h"
 #include "mpistream.h"
 #include "observer.h"
 
-MDManager::MDManager(int &argc, char **&argv) : control_synced(false) {
+MDManager::MDManager(int &argc, char **&argv) : control_synced(false), device_executors(true), routed(nullptr) {
   MPI_Init(&argc, &argv);
   MPI_Comm_size(MPI_COMM_WORLD, &num_procs);
   MPI_Comm_rank(MPI_COMM_WORLD, &rank);
@@ -41,6 +46,7 @@ MDManager::MDManager(int &argc, char **&argv) : control_synced(false) {
   const std::string prec = param.GetStringDef("Precision", "FP64");
   const int precision = (prec == "FP32Mixed" || prec == "FP32") ? MDG_FP32_MIXED : MDG_FP64;
   const int capacity = param.GetIntegerDef("Capacity", N);
+  device_executors = param.GetBooleanDef("DeviceExecutors", true);
   mdv.push_back(new MDUnit(0, sinfo, pinfo, capacity, precision));
   s_time = 0.0;
 }
@@ -137,7 +143,43 @@ void MDManager::MakePairList(void) {
 }
 
 void MDManager::ExecuteAll(Executor *ex) {
+  if (device_executors && RouteToDevice(ex)) return;
   for (size_t i = 0; i < mdv.size(); i++) mdv[i]->Execute(ex);
+}
+
+// Executors the device applies itself after every step (mdg_set_external),
+// recognised by their class name: GravityImposer (src/phaseflow.cc:58-73),
+// a uniform kick p += G dt along one axis, whose kick is read by running it
+// once on two scratch atoms.  The project calls ExecuteAll with it after
+// every Calculate(), which is when the device applies it; the first call
+// hands it to the device (steps already queued get it too, as they come
+// before that call in the project's loop) and later calls are no-ops.  Any
+// other executor, or one whose probe is not a uniform kick along one axis,
+// runs on the host mirror as in the reference.
+bool MDManager::RouteToDevice(Executor *ex) {
+  if (routed == ex) return true;
+  if (routed || mdv.size() != 1 || !mdv[0]->Device()) return false;
+  int status = 0;
+  char *name = abi::__cxa_demangle(typeid(*ex).name(), nullptr, nullptr, &status);
+  const std::string cls = (status == 0 && name) ? name : typeid(*ex).name();
+  free(name);
+  if (cls != "GravityImposer") return false;
+  double dp[D] = {0.0, 0.0, 0.0, 0.0};
+  if (!mdv[0]->ProbeUniformKick(ex, dp)) return false;
+  int axis = -1;
+  for (int d = 0; d < 3; d++)
+    if (dp[d] != 0.0) axis = (axis < 0) ? d : 3;
+  if (axis < 0 || axis > 2) return false;
+  mdg_external x;
+  memset(&x, 0, sizeof x);
+  x.kind = MDG_EXTERNAL_GRAVITY;
+  x.axis = axis;
+  x.strength = dp[axis];  // G dt, applied as strength x time_step with time_step 1
+  x.time_step = 1.0;
+  mdg_check(mdv[0]->Device(), mdg_set_external(mdv[0]->Device(), &x), "mdg_set_external");
+  routed = ex;
+  mout << "# " << cls << " runs on the device" << std::endl;
+  return true;
 }
 
 bool MDManager::IsPairListExpired(void) { return mdv[0]->IsPairListExpired(); }

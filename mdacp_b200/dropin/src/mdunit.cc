@@ -8,7 +8,7 @@
 #include "mpistream.h"
 
 MDUnit::MDUnit(int id_, SimulationInfo *si, ParaInfo *pi, int capacity, int precision_)
-    : sinfo(si), pinfo(pi), id(id_), dev(nullptr), precision(precision_) {
+    : sinfo(si), pinfo(pi), id(id_), dev(nullptr), precision(precision_), probe(nullptr) {
   vars = new Variables(capacity);
   plist = new PairList();
   int grid_size[D], grid_position[D];
@@ -28,6 +28,9 @@ MDUnit::MDUnit(int id_, SimulationInfo *si, ParaInfo *pi, int capacity, int prec
 MDUnit::~MDUnit(void) {
   if (dev) {
     vars->SyncToDevice();  // run queued steps before the state goes away
+    // the last snapshot file is written before the handle goes; a failed
+    // write stops the run as the reference's own file output would
+    mdg_check(dev, mdg_snapshot_wait(dev), "mdg_snapshot_wait");
     mdg_destroy(dev);
   }
   delete vars;
@@ -70,11 +73,32 @@ void MDUnit::SetControl(void) {
 }
 
 Variables *MDUnit::GetVariables(void) {
+  if (probe) return probe;
   // the caller may read and write the arrays: hand over a current mirror and
   // upload it again before the next device step
   vars->SyncToHost();
   vars->MarkHostDirty();
   return vars;
+}
+
+bool MDUnit::ProbeUniformKick(Executor *ex, double dp[D]) {
+  Variables scratch(4);
+  double x0[D] = {0.31 * sinfo->L[X], 0.47 * sinfo->L[Y], 0.53 * sinfo->L[Z], 0.0};
+  double x1[D] = {0.77 * sinfo->L[X], 0.19 * sinfo->L[Y], 0.61 * sinfo->L[Z], 0.0};
+  double v0[D] = {0.25, -0.5, 0.125, 0.0}, v1[D] = {-1.5, 0.75, 2.0, 0.0};
+  scratch.AddParticle(x0, v0, 0);
+  scratch.AddParticle(x1, v1, 1);
+  probe = &scratch;
+  ex->Execute(this);
+  probe = nullptr;
+  if (scratch.GetParticleNumber() != 2) return false;
+  bool uniform = true;
+  for (int d = 0; d < 3; d++) {
+    dp[d] = scratch.p[0][d] - v0[d];
+    uniform = uniform && scratch.q[0][d] == x0[d] && scratch.q[1][d] == x1[d] &&
+              scratch.p[1][d] - v1[d] == dp[d];
+  }
+  return uniform;
 }
 
 void MDUnit::AddParticle(double x[D], int type) {

@@ -10,11 +10,11 @@
 #   oracle/_ref/mdacp_rc25_plain  oracle/_ref/mdacp_rc30_plain   (-ffp-contract=off, SSE2: bit-exact oracle)
 #   oracle/_ref/mdacp_rc25_avx2   oracle/_ref/mdacp_rc30_avx2    (-DAVX2 -mavx2 -mfma: timed CPU baseline)
 #
-# Usage: oracle/ref/build_ref.sh [REFERENCE_ROOT]
+# Usage: oracle/ref/build_ref.sh REFERENCE_ROOT   (or MDACP_REFERENCE=REFERENCE_ROOT)
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 REPO="$(cd "$HERE/../.." && pwd)"
-REF="${1:-${MDACP_REFERENCE:-/root/reference}}"
+REF="${1:-${MDACP_REFERENCE:-}}"
 OUT="$REPO/oracle/_ref"
 if [ ! -f "$REF/src/mdmanager.cc" ]; then
   echo "build_ref: reference sources not found at $REF" >&2

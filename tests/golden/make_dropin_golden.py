@@ -29,6 +29,19 @@ CASES = {
                                        "AimedTemperature": "1.5", "HeatbathTau": "0.1"}),
     "collision_rc30": (3.0, {"Mode": "Collision", "SystemSize": "40", "TimeStep": "0.005",
                              "TotalLoop": "300", "ObserveLoop": "50"}),
+    # the projects whose executors run after every step: gravity on the
+    # atoms of a liquid cylinder (GravityImposer, src/phaseflow.cc:58-73) and
+    # a piston compressing a gas against a wall, then cooling it
+    # (MyPiston, src/rankine.cc:55-97); Burst thermalises and releases a
+    # droplet (its ShellForce executor, src/burst.cc:67-99, is never run)
+    "phaseflow_rc25": (2.5, {"Mode": "PhaseFlow", "SystemSize": "16", "TimeStep": "0.005",
+                             "TotalLoop": "300", "ObserveLoop": "50", "InitialVelocity": "1.0"}),
+    "rankine_rc25": (2.5, {"Mode": "Rankine", "Density": "0.2", "SystemSizeX": "16", "SystemSizeY": "16",
+                           "SystemSizeZ": "40", "TimeStep": "0.005", "TotalLoop": "500", "ObserveLoop": "50",
+                           "InitialVelocity": "1.0", "AimedTemperature": "0.5"}),
+    "burst_rc25": (2.5, {"Mode": "Burst", "Density": "0.8", "SystemSize": "24", "Radius": "6",
+                         "TimeStep": "0.005", "ThermalizeLoop": "100", "TotalLoop": "200", "ObserveLoop": "50",
+                         "InitialVelocity": "0.9"}),
     # thermalise (Nose-Hoover), ChangeScale 1.05, then bubble histograms
     # (conf%04d.dat, one byte per grid cell) every ObserveLoop steps
     "cavitation_rc25": (2.5, {"Mode": "Cavitation", "Density": "0.7", "SystemSize": "12",

@@ -79,3 +79,44 @@ def test_reference_arm_prints_once_under_torchrun():
     assert line["impl"] == "reference" and line["n_gpus"] == 2
     assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
     assert line["cpu_baseline"]["kind"] == "reference"
+
+
+def _partition_worker(rank, ws, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(ws),
+                      LOCAL_RANK=str(rank))
+    from mdacp_b200 import workloads as W
+
+    dist = bench.init_dist(ws, "gloo")
+    reps = W.config_c4(seed=404)
+    mine, loads = bench.replica_share(reps, ws, rank)
+    # stand-in per-replica metrics of this rank's share (rebuilds, energy)
+    vals = np.array([[k + 1.0, -0.5 * k] for k in mine]).reshape(len(mine), 2)
+    full = bench.gather_replica_metrics(dist, len(reps), mine, vals)
+    out.put((rank, list(mine), loads.tolist(), full.tolist(), len(reps)))
+    dist.destroy_process_group()
+
+
+def test_replica_partition_and_gather_on_gloo():
+    # one 256-replica ensemble split over 2 ranks (balanced by atoms x
+    # neighbours); every replica is owned once and the per-replica metrics
+    # of both shares reach every rank
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_partition_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = {}
+    for _ in procs:
+        rank, mine, loads, full, nrep = q.get(timeout=300)
+        got[rank] = (mine, loads, np.asarray(full), nrep)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    nrep = got[0][3]
+    owned = sorted(got[0][0] + got[1][0])
+    assert owned == list(range(nrep))
+    loads = np.asarray(got[0][1])
+    assert loads.max() / loads.mean() - 1.0 < 0.10
+    expect = np.array([[k + 1.0, -0.5 * k] for k in range(nrep)])
+    assert np.array_equal(got[0][2], expect) and np.array_equal(got[1][2], expect)
