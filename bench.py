@@ -199,13 +199,22 @@ def main():
                     help="restrict the timed runs (profiling); the JSON line needs both")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end run (profiling)")
     ap.add_argument("--no-force-error", action="store_true", help="skip the FP32-vs-FP64 force check")
-    ap.add_argument("--drift-steps", type=int, default=2000,
-                    help="NVE steps of the energy-drift comparison of the two paths (0: skip)")
+    ap.add_argument("--drift-steps", type=int, default=10000,
+                    help="NVE steps of the energy-drift comparison of the two paths (0: skip); the 2.05M-atom "
+                         "configuration's run is 10,000 steps")
     ap.add_argument("--stage-atoms", type=int, default=0,
                     help="FP32-mixed force: partner positions staged per 128-atom block in shared memory, "
                          "at most this many atoms (0: gather from global memory, the default; -1: 2304)")
     ap.add_argument("--eager", action="store_true",
                     help="launch every kernel from the host instead of CUDA graphs (for profilers)")
+    ap.add_argument("--threads-per-atom", type=int, default=0,
+                    help="FP32-mixed force pass lanes per atom (0: tuned at the first step)")
+    ap.add_argument("--build-block", type=int, default=0, help="list build threads per block (0: tuned)")
+    ap.add_argument("--build-lanes", type=int, default=0, help="list build lanes per atom (0: tuned)")
+    ap.add_argument("--step-mode", choices=["auto", "graphs", "persistent"], default="auto",
+                    help="FP32-mixed NVE steps as CUDA graphs or one persistent launch (auto: by size)")
+    ap.add_argument("--adjoint-launches", action="store_true",
+                    help="c5 profiling: two 40-step gradient runs (checkpoints every 20 steps) and nothing else")
     ap.add_argument("--config", choices=["c2", "c1", "c3", "c4", "c5"], default="c2",
                     help="c2: 2.05M-atom liquid (headline); c1: 32k atoms rho 0.5; c3: 1M-atom Langevin slab; "
                          "c4: 256-replica ensemble; c5: adjoint gradients of a 32k-atom trajectory")
@@ -225,6 +234,12 @@ def main():
         return main_reference(args, ws, rank, state, config)
     if args.stage_atoms != 0:
         config["force_stage_atoms"] = args.stage_atoms
+    for key, val in (("threads_per_atom", args.threads_per_atom), ("build_block", args.build_block),
+                     ("build_threads_per_atom", args.build_lanes)):
+        if val:
+            config.setdefault("pinned_shapes", {})[key] = val
+    if args.step_mode != "auto":
+        config["step_mode"] = {"graphs": 1, "persistent": 2}[args.step_mode]
     return main_mdg(args, ws, rank, local, state, config)
 
 
@@ -269,6 +284,9 @@ def metric_for(config):
 def system_kwargs(state, config, M):
     kw = dict(cutoff=state.rc, time_step=state.dt, capacity=state.n,
               stage_atoms=config.get("force_stage_atoms", 0))
+    if config.get("step_mode") is not None:
+        kw["step_mode"] = config["step_mode"]
+    kw.update(config.get("pinned_shapes", {}))
     if config.get("thermostat") == "Langevin":
         kw.update(thermostat=M.LANGEVIN, aimed_temperature=config["temperature"],
                   heatbath_gamma=config["gamma"], seed=7)
@@ -296,6 +314,14 @@ def main_reference(args, ws, rank, state, config):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def force_errors(f, f_ref):
+    """Norm-wise max and RMS relative force error."""
+    d = np.linalg.norm(f - f_ref, axis=1)
+    mag = np.linalg.norm(f_ref, axis=1)
+    return {"max": float(d.max() / max(mag.max(), np.sqrt((mag ** 2).mean()))),
+            "rms": float(np.sqrt((d ** 2).mean()) / np.sqrt((mag ** 2).mean()))}
 
 
 def force_kernel_bytes(n, list_entries, precision):
@@ -412,18 +438,14 @@ def main_mdg(args, ws, rank, local, state, config):
     sa = M.System(state.L, precision=M.FP64, device=local, **system_kwargs(state, config, M))
     sa.set_state(state.q, state.v)
     sa.calculate(50)
-    q, v = sa.state_by_id()
+    q, v_state = sa.state_by_id()
     f64 = sa.forces_by_id()
     sa.close()
     sb = M.System(state.L, precision=M.FP32_MIXED, device=local, **system_kwargs(state, config, M))
-    sb.set_state(q, v)
+    sb.set_state(q, v_state)
     f32 = sb.forces_by_id()
     sb.close()
-    d = np.linalg.norm(f32 - f64, axis=1)
-    mag = np.linalg.norm(f64, axis=1)
-    errs = {"max": float(d.max() / max(mag.max(), np.sqrt((mag ** 2).mean()))),
-            "rms": float(np.sqrt((d ** 2).mean()) / np.sqrt((mag ** 2).mean())),
-            "state": "after 50 FP64 steps from the start state"}
+    errs = dict(force_errors(f32, f64), state="after 50 FP64 steps from the start state")
 
     # NVE energy drift of both paths from the same state (total energy per atom
     # observed every 100 MD steps)
@@ -453,6 +475,19 @@ def main_mdg(args, ws, rank, local, state, config):
     rebuilds = r32["info1"]["rebuilds"] - r32["info0"]["rebuilds"]
     entries = r32["info1"]["list_entries"]
     fbytes = force_kernel_bytes(n, entries, "fp32")
+    roofline_note = "force kernel timed with CUDA events around every launch of the timed region"
+    if r32["force_launches"] == 0:
+        # the timed steps ran in the persistent multi-step pass, which has no
+        # separate force launches: time the same pass launched per step
+        kw = dict(system_kwargs(state, config, M), step_mode=M.STEPS_GRAPHS)
+        sg = M.System(state.L, precision=M.FP32_MIXED, device=local, **kw)
+        sg.set_state(state.q, state.v)
+        gargs = argparse.Namespace(**dict(vars(args), steps=min(args.steps, 3), warmup=min(args.warmup, 3)))
+        _, fms_g, fl_g, _, _, _ = timed_run(sg, gargs, None, device, torch)
+        sg.close()
+        r32 = dict(r32, force_ms=fms_g, force_launches=fl_g)
+        roofline_note = ("the timed steps ran in the persistent multi-step pass; its force pass was timed "
+                         "launched once per step (CUDA graphs) on the same system")
     f_avg_ms = r32["force_ms"] / max(1, r32["force_launches"])
     achieved = fbytes / (f_avg_ms * 1e-3) / 1e9
     traffic = None
@@ -468,8 +503,10 @@ def main_mdg(args, ws, rank, local, state, config):
                        rebuilds=rebuilds, mean_row=entries / n,
                        tuned={"threads_per_atom": r32["info1"]["threads_per_atom"],
                               "build_block": r32["info1"]["build_block"],
-                              "fp64_build_block": r64["info1"]["build_block"],
-                              "how": "timed once per device and problem shape at the first step"}),
+                              "build_threads_per_atom": r32["info1"]["build_threads_per_atom"],
+                              "fp64_build": [r64["info1"]["build_block"], r64["info1"]["build_threads_per_atom"]],
+                              "how": "timed once per device and problem shape at the first step"},
+                       persistent_steps=r32["info1"]["persistent_steps"] - r32["info0"]["persistent_steps"]),
         "fp64": {"value": r64["value"], "ms_per_md_step": r64["ms"] / (args.steps * args.md_steps_per_step),
                  "speedup_fp32_over_fp64": r32["value"] / r64["value"]},
         "ms_per_md_step": r32["ms"] / (args.steps * args.md_steps_per_step),
@@ -482,7 +519,7 @@ def main_mdg(args, ws, rank, local, state, config):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "kernel": "k_force_fp32 (fused NVE step: drift, kick, drift, pack)",
                      "algorithmic_bytes_per_launch": fbytes, "avg_launch_ms": f_avg_ms,
-                     "launches": r32["force_launches"], "peak_kind": peak_kind},
+                     "launches": r32["force_launches"], "peak_kind": peak_kind, "timing": roofline_note},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 32 * n,
                 "d2h_bytes_per_step": 2 * 32 * n},
         "gpu_launches": r32["launches"],
@@ -498,6 +535,23 @@ def main_mdg(args, ws, rank, local, state, config):
         except Exception as exc:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                                     "sample": f"not run: {exc}"}
+        # the checker: both GPU paths' forces at the same state against the
+        # CPU oracle's FP64 forces (the reference's arithmetic)
+        try:
+            from oracle import lj_oracle as O
+
+            o = O.Oracle(q, v_state, state.ids, state.L, state.rc, state.dt)
+            o.make_pairlist()
+            of = o.forces()
+            _, _, oid = o.state()
+            o.close()
+            f_or = np.empty_like(of)
+            f_or[oid] = of
+            line["force_error_vs_oracle"] = {"fp32_mixed": force_errors(f32, f_or), "fp64": force_errors(f64, f_or),
+                                             "state": errs["state"],
+                                             "oracle": "oracle/lj_oracle.c, the reference's FP64 arithmetic"}
+        except Exception as exc:  # noqa: BLE001
+            line["force_error_vs_oracle"] = {"not_run": str(exc)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -518,6 +572,19 @@ def main_adjoint(args, ws, rank, local):
     device = f"cuda:{local}"
     torch.cuda.set_device(local)
     st = W.config_c5(seed=55 + rank)
+    if args.adjoint_launches:
+        # the sequence of profiles/adjoint_lj32000_launches.md: the
+        # lanes-per-atom autotuner and warm-up, then one 40-step gradient run
+        kw = dict(steps=40, checkpoint_every=20, time_step=st.dt, device=local)
+        A.trajectory_gradients(st.q, st.v, st.L, **kw)
+        t0 = time.perf_counter()
+        A.trajectory_gradients(st.q, st.v, st.L, **kw)
+        if rank == 0:
+            print(json.dumps({"profiling_run": "adjoint, 32000 atoms, 40 steps",
+                              "seconds": time.perf_counter() - t0}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
     n, T, k = st.n, 200, 20
     kw = dict(steps=T, checkpoint_every=k, time_step=st.dt, device=local)
     per_tpa = {}

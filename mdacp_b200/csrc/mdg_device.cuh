@@ -154,6 +154,11 @@ __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a,
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
 
+// The skin budget's cost of one step, 2 vmax dt, each operation separately
+// rounded as in PairList::IsPairListExpired (src/pairlist.cc:25-65), so
+// every kernel that spends the budget spends the same amount.
+__device__ __forceinline__ double skin_cost(double vmax, double dt) { return dmul(dmul(vmax, 2.0), dt); }
+
 __device__ __forceinline__ void atomic_max_double_bits(unsigned long long *addr, double v) {
   // non-negative doubles order like their bit patterns
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
@@ -274,11 +279,11 @@ static __global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_di
     } else {
       if (st->budget > 0.0) {
         const double vmax = sqrt(__longlong_as_double((long long)st->vmax2_bits));
-        if (vmax * 2.0 * b.dt > b.buffer_length) {
+        if (skin_cost(vmax, b.dt) > b.buffer_length) {
           st->too_fast_v = vmax;
           atomicOr(&st->error, kErrTooFast);
         } else {
-          st->budget = st->budget - vmax * 2.0 * b.dt;
+          st->budget = dsub(st->budget, skin_cost(vmax, b.dt));
         }
       }
       if (st->error == 0 && st->budget < 0.0) {
@@ -1850,8 +1855,8 @@ constexpr long long kBarrierPolls = 16000000ll;
 __device__ __forceinline__ bool take_step_alone(Status *st, const Box &b) {
   if (st->error || st->list_stale || !(st->budget > 0.0)) return false;
   const double vmax = sqrt(__longlong_as_double((long long)st->vmax2_bits));
-  if (vmax * 2.0 * b.dt > b.buffer_length) return false;  // k_expiry reports the too-fast atom
-  const double budget = st->budget - vmax * 2.0 * b.dt;
+  if (skin_cost(vmax, b.dt) > b.buffer_length) return false;  // k_expiry reports the too-fast atom
+  const double budget = dsub(st->budget, skin_cost(vmax, b.dt));
   if (budget < 0.0) return false;
   st->budget = budget;
   st->vmax2_bits = 0ull;

@@ -235,8 +235,8 @@ __global__ void ke_expiry(Ens e, cudaGraphConditionalHandle h_disp, int in_graph
       } else {
         if (st.budget > 0.0) {
           const double vmax = sqrt(__longlong_as_double((long long)st.vmax2_bits));
-          if (vmax * 2.0 * e.dt > e.buffer_length) atomicOr(e.error, kErrTooFast);
-          else st.budget = st.budget - vmax * 2.0 * e.dt;
+          if (skin_cost(vmax, e.dt) > e.buffer_length) atomicOr(e.error, kErrTooFast);
+          else st.budget = dsub(st.budget, skin_cost(vmax, e.dt));
         }
         if (st.budget < 0.0) {
           disp = 1;
