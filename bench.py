@@ -540,7 +540,12 @@ def main_mdg(args, ws, rank, local, state, config):
         try:
             from oracle import lj_oracle as O
 
-            o = O.Oracle(q, v_state, state.ids, state.L, state.rc, state.dt)
+            # positions drift out of the box between rebuilds; the oracle, as the
+            # reference's AddParticle, keeps only atoms inside it: wrap them once
+            # as the device's rebuild does
+            L = np.asarray(state.L)
+            qw = np.where(q < 0.0, q + L, np.where(q > L, q - L, q))
+            o = O.Oracle(qw, v_state, state.ids, state.L, state.rc, state.dt)
             o.make_pairlist()
             of = o.forces()
             _, _, oid = o.state()

@@ -113,6 +113,16 @@ mdg_status mdg_set_state(mdg_handle *h, const double *q4, const double *v4, cons
    of Variables::q/p/type.  Arrays are in the current slot order. */
 mdg_status mdg_get_state(mdg_handle *h, double *q4, double *v4, int *type, int n);
 mdg_status mdg_get_ids(mdg_handle *h, int *ids, int n);
+/* Replaces: an Executor's writes to Variables::p between steps
+   (MDManager::ExecuteAll, src/mdmanager.cc:586-592; e.g. GravityImposer,
+   src/phaseflow.cc:58-73, MyPiston, src/rankine.cc:55-97): new velocities,
+   n x 4 doubles in the current slot order (the order mdg_get_state returns),
+   positions untouched.  Unlike mdg_set_state it keeps the list, the skin
+   budget and the observers' ghost age, as the reference's executors leave
+   its PairList and ghost copies alone; the |v| maximum of the next skin test
+   is taken from the new velocities (IsPairListExpired reads the momenta
+   after the executor). */
+mdg_status mdg_set_velocities(mdg_handle *h, const double *v4, int n);
 mdg_status mdg_particle_number(mdg_handle *h, int *n);
 
 /* Replaces: MDManager::MakePairList (src/mdmanager.cc:387-417): wrap into

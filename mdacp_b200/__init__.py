@@ -226,6 +226,7 @@ SIGNATURES = {
     "mdg_slabs_forces": (ctypes.c_int, [_H, _DP, ctypes.c_int]),
     "mdg_slabs_info": (ctypes.c_int, [_H, _I64P, _I64P, _IP, _IP]),
     "mdg_slabs_last_error": (ctypes.c_char_p, [_H]),
+    "mdg_set_velocities": (ctypes.c_int, [_H, _DP, ctypes.c_int]),
     "mdg_partition_replicas": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _IP,
                                               _DP]),
     "mdg_ensemble_set_kernel_timing": (ctypes.c_int, [_H, ctypes.c_int]),
@@ -351,6 +352,11 @@ class System:
         t = _i(type_) if type_ is not None else None
         self._check(self.lib.mdg_set_state(self.h, _d(q4), _d(v4), t, n))
         self.n = n
+
+    def set_velocities4(self, v4):
+        """New velocities in the current slot order, (n,4) float64 (mdg_set_velocities)."""
+        v4 = np.ascontiguousarray(v4, dtype=np.float64)
+        self._check(self.lib.mdg_set_velocities(self.h, _d(v4), v4.shape[0]))
 
     def get_state4(self, q4, v4, type_=None):
         t = _i(type_) if type_ is not None else None

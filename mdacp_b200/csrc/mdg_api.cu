@@ -668,8 +668,15 @@ mdg_status autotune(mdg_handle *h) {
       return MDG_OK;
     }
   }
-  mdg_status r = ensure_list(h);
+  // the tuner needs a list; a handle whose list is stale (no build since its
+  // state was set: the reference's uninitialised PairList, which rebuilds at
+  // the first step without spending the skin budget) gets its status back
+  // afterwards, so that the first step behaves the same whether the shapes
+  // were timed, cached or pinned
+  Status before;
+  mdg_status r = read_status(h, &before);
   if (r) return r;
+  if ((r = ensure_list(h))) return r;
   cudaStream_t s = h->stream;
   const int n = h->n;
   int tpa = h->tpa, bb = h->build_block;
@@ -719,6 +726,10 @@ mdg_status autotune(mdg_handle *h) {
   Status st;
   if ((r = read_status(h, &st))) return r;
   if (st.error) return translate_device_error(h, st);
+  if (before.list_stale && !before.error) {
+    CUDA_TRY(h, cudaMemcpyAsync(h->a.st, &before, sizeof(Status), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  }
   h->tpa = tpa;
   h->build_block = bb;
   h->build_tpa = bl;
@@ -1010,6 +1021,24 @@ mdg_status mdg_get_state(mdg_handle *h, double *q4, double *v4, int *type, int n
   if (v4) CUDA_TRY(h, cudaMemcpyAsync(v4, h->a.v, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
   if (type) CUDA_TRY(h, cudaMemcpyAsync(type, h->a.type, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return MDG_OK;
+}
+
+mdg_status mdg_set_velocities(mdg_handle *h, const double *v4, int n) {
+  mdg_status r = check_ready(h);
+  if (r) return r;
+  if (n != h->n || (n > 0 && !v4)) return fail(h, MDG_ERR_INVALID_ARGUMENT, "n differs from the handle's atom count");
+  if (n == 0) return MDG_OK;
+  CUDA_TRY(h, cudaSetDevice(h->prm.device));
+  h->fix_buf = -1;  // the fused step's packed first-drift copy used the old velocities
+  const unsigned long long zero = 0ull;
+  CUDA_TRY(h, cudaMemcpyAsync(h->a.v, v4, sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->vmax2_bits, &zero, sizeof zero, cudaMemcpyHostToDevice, h->stream));
+  k_vmax<kBlock><<<blocks_for(n, kBlock), kBlock, 0, h->stream>>>(h->a, n);
+  CUDA_TRY(h, cudaGetLastError());
+  Status st;
+  if ((r = read_status(h, &st))) return r;
+  if (st.error) return translate_device_error(h, st);
   return MDG_OK;
 }
 

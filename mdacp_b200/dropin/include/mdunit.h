@@ -82,9 +82,10 @@ class MDUnit {
   mdg_handle *Device(void) { return dev; }
   Variables *Vars(void) { return vars; }
   void SetControl(void);
-  // Runs ex once on two scratch atoms (different positions and momenta)
-  // instead of the unit's own: true, with the change of p in dp, if ex
-  // added the same dp to both and moved neither -- a uniform kick.
+  // Runs ex on two scratch atoms (at different places, first at rest, then
+  // moving) instead of the unit's own: true, with the change of p in dp, if
+  // ex gave both the same kick whatever their place and velocity and moved
+  // neither -- a uniform kick (dp as read from the atoms at rest).
   bool ProbeUniformKick(Executor *ex, double dp[D]);
 };
 #endif

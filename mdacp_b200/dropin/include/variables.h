@@ -21,6 +21,7 @@ class Variables {
   double C0, C2;
   mdg_handle *device;     // GPU state (owned by MDUnit)
   bool host_dirty;        // host arrays changed since the last upload
+  bool momenta_dirty;     // only p changed since the last upload (an executor's kick)
   bool device_newer;      // device state advanced since the last download
   long pending_steps;     // MDManager::Calculate calls not yet run on the device
 
@@ -54,6 +55,13 @@ class Variables {
   void AttachDevice(mdg_handle *h) { device = h; host_dirty = true; device_newer = false; }
   mdg_handle *Device(void) { return device; }
   void MarkHostDirty(void) { host_dirty = true; }
+  // The host changed p only (positions, atom count and order as downloaded):
+  // the upload replaces the velocities and keeps the device's list, skin
+  // budget and ghost age (mdg_set_velocities).
+  void MarkMomentaDirty(void) {
+    host_dirty = false;
+    momenta_dirty = true;
+  }
   void MarkDeviceNewer(void) { device_newer = true; }
   void QueueSteps(long n) { pending_steps += n; }
   // Runs queued steps, uploads host changes: after this the device is current.

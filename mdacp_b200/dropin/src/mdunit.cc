@@ -2,7 +2,10 @@
 // one unit spanning the whole periodic box, backed by one GPU handle.
 #include "mdunit.h"
 
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
+#include <vector>
 #include <cstring>
 
 #include "mpistream.h"
@@ -82,23 +85,41 @@ Variables *MDUnit::GetVariables(void) {
 }
 
 bool MDUnit::ProbeUniformKick(Executor *ex, double dp[D]) {
-  Variables scratch(4);
-  double x0[D] = {0.31 * sinfo->L[X], 0.47 * sinfo->L[Y], 0.53 * sinfo->L[Z], 0.0};
-  double x1[D] = {0.77 * sinfo->L[X], 0.19 * sinfo->L[Y], 0.61 * sinfo->L[Z], 0.0};
-  double v0[D] = {0.25, -0.5, 0.125, 0.0}, v1[D] = {-1.5, 0.75, 2.0, 0.0};
-  scratch.AddParticle(x0, v0, 0);
-  scratch.AddParticle(x1, v1, 1);
-  probe = &scratch;
-  ex->Execute(this);
-  probe = nullptr;
-  if (scratch.GetParticleNumber() != 2) return false;
-  bool uniform = true;
-  for (int d = 0; d < 3; d++) {
-    dp[d] = scratch.p[0][d] - v0[d];
-    uniform = uniform && scratch.q[0][d] == x0[d] && scratch.q[1][d] == x1[d] &&
-              scratch.p[1][d] - v1[d] == dp[d];
+  // two atoms at rest at different places: the kick each gets is exact (0 + k)
+  // and must be the same; two moving atoms: the same kick up to the rounding
+  // of v + k - v, and no atom may move
+  const double xs[2][D] = {{0.31 * sinfo->L[X], 0.47 * sinfo->L[Y], 0.53 * sinfo->L[Z], 0.0},
+                           {0.77 * sinfo->L[X], 0.19 * sinfo->L[Y], 0.61 * sinfo->L[Z], 0.0}};
+  const double vs[2][D] = {{0.25, -0.5, 0.125, 0.0}, {-1.5, 0.75, 2.0, 0.0}};
+  double kick[2][2][D];
+  for (int moving = 0; moving < 2; moving++) {
+    Variables scratch(4);
+    for (int a = 0; a < 2; a++) {
+      double x[D], v[D];
+      for (int d = 0; d < D; d++) {
+        x[d] = xs[a][d];
+        v[d] = moving ? vs[a][d] : 0.0;
+      }
+      scratch.AddParticle(x, v, a);
+    }
+    probe = &scratch;
+    ex->Execute(this);
+    probe = nullptr;
+    if (scratch.GetParticleNumber() != 2) return false;
+    for (int a = 0; a < 2; a++)
+      for (int d = 0; d < 3; d++) {
+        if (scratch.q[a][d] != xs[a][d]) return false;
+        kick[moving][a][d] = scratch.p[a][d] - (moving ? vs[a][d] : 0.0);
+      }
   }
-  return uniform;
+  for (int d = 0; d < 3; d++) {
+    dp[d] = kick[0][0][d];
+    if (kick[0][1][d] != dp[d]) return false;
+    const double tol = 1e-12 * std::fabs(dp[d]) + 1e-15 * 4.0;
+    for (int a = 0; a < 2; a++)
+      if (std::fabs(kick[1][a][d] - dp[d]) > tol) return false;
+  }
+  return true;
 }
 
 void MDUnit::AddParticle(double x[D], int type) {
@@ -143,8 +164,18 @@ double MDUnit::ObserveDouble(DoubleObserver *obs) {
 
 void MDUnit::Execute(Executor *ex) {
   vars->SyncToHost();
+  // an executor that leaves positions and atoms alone (the reference's
+  // gravity, piston and shell wall change momenta only) goes up as new
+  // velocities, which keeps the list and the skin budget as the reference's
+  // PairList keeps them; any other change uploads the whole state
+  const int pn = vars->GetParticleNumber();
+  std::vector<double> q0(&vars->q[0][0], &vars->q[0][0] + (size_t)D * pn);
+  std::vector<int> t0(vars->type, vars->type + pn);
   ex->Execute(this);
-  vars->MarkHostDirty();
+  const bool same = vars->GetParticleNumber() == pn &&
+                    std::equal(q0.begin(), q0.end(), &vars->q[0][0]) && std::equal(t0.begin(), t0.end(), vars->type);
+  if (same) vars->MarkMomentaDirty();
+  else vars->MarkHostDirty();
 }
 
 void MDUnit::MakePairList(void) {

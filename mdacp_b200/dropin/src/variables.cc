@@ -24,7 +24,7 @@ Variables::Variables(void) : Variables(N) {}
 
 Variables::Variables(int capacity_)
     : particle_number(0), total_particle_number(0), capacity(capacity_), device(nullptr),
-      host_dirty(false), device_newer(false), pending_steps(0), Zeta(0.0), SimulationTime(0.0) {
+      host_dirty(false), momenta_dirty(false), device_newer(false), pending_steps(0), Zeta(0.0), SimulationTime(0.0) {
   // smoothed-LJ constants (src/variables.cc:21-27)
   const double s2 = 1.0 / (CUTOFF_LENGTH * CUTOFF_LENGTH);
   const double s6 = s2 * s2 * s2;
@@ -168,6 +168,11 @@ void Variables::SyncToDevice(void) {
     mdg_check(device, mdg_set_state(device, &q[0][0], &p[0][0], type, particle_number), "mdg_set_state");
     mdg_check(device, mdg_set_zeta(device, Zeta), "mdg_set_zeta");
     host_dirty = false;
+    momenta_dirty = false;
+    device_newer = false;
+  } else if (momenta_dirty) {
+    mdg_check(device, mdg_set_velocities(device, &p[0][0], particle_number), "mdg_set_velocities");
+    momenta_dirty = false;
     device_newer = false;
   }
   if (pending_steps > 0) {

@@ -828,3 +828,54 @@ void ljo_observe(const ljo_system *s, double *ke, double *pe, double *virial) {
   if (pe) *pe = energy;
   if (virial) *virial = phi / 3.0;
 }
+
+/* Neumaier's compensated sum (a running sum plus a correction term): the
+   checker's own summation error stays near one rounding however many terms
+   are added, where a plain running sum of n terms can drift by up to n
+   roundings when the terms are alike (a lattice). */
+typedef struct { double s, c; } ljo_csum;
+static void csum_add(ljo_csum *a, double x) {
+  const double t = a->s + x;
+  if (fabs(a->s) >= fabs(x)) a->c += (a->s - t) + x;
+  else a->c += (x - t) + a->s;
+  a->s = t;
+}
+
+/* The sums of ljo_observe, each term formed exactly as there (the reference's
+   expression trees), added with compensation.  Test infrastructure: the
+   checker for sums over millions of pairs, where the reference's own running
+   sum carries more rounding than the 1e-12 parity bar allows. */
+void ljo_observe_compensated(const ljo_system *s, double *ke, double *pe, double *virial) {
+  const double CL2 = s->prm.rc * s->prm.rc;
+  const double C2 = s->c2, C0 = s->c0;
+  const int pn = s->pn;
+  ljo_csum energy = {0.0, 0.0}, phi = {0.0, 0.0}, kin = {0.0, 0.0};
+  for (int64_t k = 0; k < s->kp_key.n; k++) {
+    const int i = s->kp_key.v[k], j = s->kp_partner.v[k];
+    double dx = s->q[i][0] - s->q[j][0];
+    double dy = s->q[i][1] - s->q[j][1];
+    double dz = s->q[i][2] - s->q[j][2];
+    const double r2 = (dx * dx + dy * dy + dz * dz);
+    if (r2 > CL2) continue;
+    double e = 4.0 * (1.0 / (r2 * r2 * r2 * r2 * r2 * r2) - 1.0 / (r2 * r2 * r2) + C2 * r2 + C0);
+    if (i >= pn || j >= pn) e *= 0.5;
+    csum_add(&energy, e);
+  }
+  for (int64_t k = 0; k < s->kp_key.n; k++) {
+    const int i = s->kp_key.v[k], j = s->kp_partner.v[k];
+    double dx = s->q[j][0] - s->q[i][0];
+    double dy = s->q[j][1] - s->q[i][1];
+    double dz = s->q[j][2] - s->q[i][2];
+    const double r2 = (dx * dx + dy * dy + dz * dz);
+    if (r2 > CL2) continue;
+    const double r6 = r2 * r2 * r2;
+    double df = ((24.0 * r6 - 48.0) / (r6 * r6 * r2) + C2 * 8.0) * r2;
+    if (i >= pn || j >= pn) df *= 0.5;
+    csum_add(&phi, df);
+  }
+  for (int i = 0; i < pn; i++)
+    for (int d = 0; d < 3; d++) csum_add(&kin, 0.5 * s->p[i][d] * s->p[i][d]);
+  if (ke) *ke = kin.s + kin.c;
+  if (pe) *pe = energy.s + energy.c;
+  if (virial) *virial = (phi.s + phi.c) / 3.0;
+}

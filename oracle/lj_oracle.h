@@ -76,6 +76,8 @@ int64_t ljo_get_pairs(const ljo_system *s, int32_t *key_id, int32_t *partner_id,
 void ljo_forces(ljo_system *s, double *f);
 /* Sums as the observers return them: KE = sum 1/2 p^2, PE, virial = sum(...)/3. */
 void ljo_observe(const ljo_system *s, double *ke, double *pe, double *virial);
+/* The same sums with compensated summation (the checker for very long sums). */
+void ljo_observe_compensated(const ljo_system *s, double *ke, double *pe, double *virial);
 
 /* Executors the reference's projects run after each Calculate() (real atoms,
    momenta = velocities): kind 1 GravityImposer (src/phaseflow.cc:58-73),

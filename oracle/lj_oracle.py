@@ -87,6 +87,7 @@ def load_library() -> ctypes.CDLL:
     lib.ljo_get_pairs.restype = ctypes.c_int64
     lib.ljo_forces.argtypes = [ctypes.c_void_p, dp]
     lib.ljo_observe.argtypes = [ctypes.c_void_p, dp, dp, dp]
+    lib.ljo_observe_compensated.argtypes = [ctypes.c_void_p, dp, dp, dp]
     lib.ljo_philox4x32.argtypes = [P(ctypes.c_uint32), P(ctypes.c_uint32), P(ctypes.c_uint32)]
     lib.ljo_langevin_normals.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, dp]
     lib.ljo_apply_external.argtypes = [ctypes.c_void_p, P(External)]
@@ -182,11 +183,15 @@ class Oracle:
         self.lib.ljo_forces(self.h, _dptr(f))
         return f
 
-    def observe(self):
+    def observe(self, compensated=False):
+        """(KE, PE, virial) as the reference sums them; compensated=True adds
+        the same terms with compensated summation (for sums over millions of
+        pairs)."""
         ke = ctypes.c_double()
         pe = ctypes.c_double()
         vir = ctypes.c_double()
-        self.lib.ljo_observe(self.h, ctypes.byref(ke), ctypes.byref(pe), ctypes.byref(vir))
+        fn = self.lib.ljo_observe_compensated if compensated else self.lib.ljo_observe
+        fn(self.h, ctypes.byref(ke), ctypes.byref(pe), ctypes.byref(vir))
         return ke.value, pe.value, vir.value
 
 

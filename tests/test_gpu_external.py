@@ -132,3 +132,30 @@ def test_invalid_executor_rejected():
         s.set_external(kind=7)
     with pytest.raises(M.MdgError):
         s.set_external(kind=M.EXTERNAL_GRAVITY, axis=3)
+
+
+def test_host_kick_through_set_velocities_equals_device_gravity():
+    # an executor that changes momenta only, run on the host between steps
+    # and uploaded with mdg_set_velocities, keeps the list and the skin
+    # budget: the trajectory equals the device executor's bit for bit, with
+    # the same rebuild steps
+    g = W.fcc_liquid(6, 0.5, 1.0, seed=91, jitter=0.05, rc=2.5, dt=0.005)
+    kick = 0.2 * 0.005
+    a = M.System(g.L, cutoff=g.rc, time_step=g.dt, capacity=g.n)
+    a.set_state(g.q, g.v)
+    a.set_external(M.EXTERNAL_GRAVITY, axis=0, strength=kick, time_step=1.0)
+    b = M.System(g.L, cutoff=g.rc, time_step=g.dt, capacity=g.n)
+    b.set_state(g.q, g.v)
+    a.calculate(60)
+    for _ in range(60):
+        b.calculate(1)
+        q4 = np.empty((b.n, 4))
+        v4 = np.empty((b.n, 4))
+        b.get_state4(q4, v4)
+        v4[:, 0] += kick
+        b.set_velocities4(v4)
+    qa, va = a.state_by_id()
+    qb, vb = b.state_by_id()
+    assert np.array_equal(qa, qb) and np.array_equal(va, vb)
+    ia, ib = a.info(), b.info()
+    assert ia["rebuilds"] == ib["rebuilds"] and ia["displacement_checks"] == ib["displacement_checks"]

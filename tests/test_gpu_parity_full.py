@@ -17,7 +17,11 @@ Forces on a perfect lattice cancel to rounding noise, so the force checks
 run on the state the oracle reaches after a few steps (handed to fresh GPU
 handles), while pair sets and observer sums are also checked at the start.
 Pair sets are compared as sorted int64 keys (key * n + partner), which
-keeps the 160-million-entry sets of the 2.05M-atom liquid cheap."""
+keeps the 160-million-entry sets of the 2.05M-atom liquid cheap.  The
+oracle's energy and virial are its pair terms added with compensated
+summation: the reference's plain running sum over 80 million pair terms of
+a lattice (nearly equal terms, correlated roundings) is itself off by
+about 4e-10 relative, above the bar."""
 from __future__ import annotations
 
 import numpy as np
@@ -66,7 +70,7 @@ def check_state(st, q, v, oracle_kw=None, fp32=True):
     del ok, op
     _, _, oid = o.state()
     f_ref = by_id(o.forces(), oid)
-    oke, ope, ovir = o.observe()
+    oke, ope, ovir = o.observe(compensated=True)
     o.close()
 
     s = gpu_system(st, q, v, M.FP64)
