@@ -140,7 +140,7 @@ cudaError_t dalloc(T **p, size_t count) {
 
 void free_arrays(Arrays &a) {
   void *ptrs[] = {a.q, a.v, a.q_old, a.qfix, a.qfix2, a.qloc, a.cxyz, a.xsub, a.ids, a.type, a.cell, a.nbr, a.nnbr, a.cell_count,
-                  a.cell_start, a.slot, a.perm, a.perm2, a.q_tmp, a.v_tmp, a.ids_tmp, a.type_tmp,
+                  a.cell_start, a.slot, a.perm, a.perm2, a.q_tmp, a.v_tmp, a.v_lag, a.ids_tmp, a.type_tmp,
                   a.cell_tmp, a.mult, a.cand, a.partials, a.st, a.stage_rng, a.stage_n, a.nbr16};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -332,17 +332,20 @@ cudaError_t set_stage_smem(int atoms) {
 }
 
 // The FP32-mixed force pass with TPA lanes per atom (drift as below).
+// Blocks hold kForceBlock atoms whatever TPA is, so the Nose-Hoover kinetic
+// energy partials cover the same atoms as k_zeta expects.
 template <int MODE, int TPA>
 void launch_fp32(mdg_handle *h, cudaStream_t s, const Thermo &th, int drift, const int4 *qf, int4 *qf_next) {
+  constexpr int kThreads = kForceBlock * TPA;
   const int n = h->n;
-  const int nb = (int)(((long long)n * TPA + kForceBlock - 1) / kForceBlock);
-  if (nb == 0) return;
+  if (n == 0) return;
+  const int nb = blocks_for(n, kForceBlock);
   if (drift == 2)
-    k_force_fp32<kForceBlock, MODE, 2, TPA><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, qf_next);
+    k_force_fp32<kThreads, MODE, 2, TPA><<<nb, kThreads, 0, s>>>(h->a, h->box, n, th, qf, qf_next);
   else if (drift)
-    k_force_fp32<kForceBlock, MODE, 1, TPA><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, nullptr);
+    k_force_fp32<kThreads, MODE, 1, TPA><<<nb, kThreads, 0, s>>>(h->a, h->box, n, th, qf, nullptr);
   else
-    k_force_fp32<kForceBlock, MODE, 0, TPA><<<nb, kForceBlock, 0, s>>>(h->a, h->box, n, th, qf, nullptr);
+    k_force_fp32<kThreads, MODE, 0, TPA><<<nb, kThreads, 0, s>>>(h->a, h->box, n, th, qf, nullptr);
 }
 
 // drift: 1 also applies the second half drift in the same pass, 2 the whole
@@ -773,7 +776,8 @@ mdg_status launch_persistent(mdg_handle *h, int steps, int *taken) {
   CUDA_TRY(h, cudaMemsetAsync(h->d_bar, 0, sizeof(GridBarrier), h->stream));
   int n = h->n, parity = h->fix_buf > 0 ? 1 : 0;
   int4 *q0 = h->a.qfix, *q1 = h->a.qfix2;
-  void *args[] = {&h->a, &h->box, &n, &steps, &q0, &q1, &parity, &h->d_bar, &h->d_pout};
+  double lag = step_lag(h);  // the ghost copies' age at a step's displacement check
+  void *args[] = {&h->a, &h->box, &n, &steps, &q0, &q1, &parity, &lag, &h->d_bar, &h->d_pout};
   CUDA_TRY(h, cudaLaunchCooperativeKernel((const void *)k_nve_persistent<kForceBlock, TPA>, dim3(grid),
                                           dim3(kForceBlock), args, 0, h->stream));
   int out[2] = {0, 0};
@@ -902,6 +906,7 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   if (e == cudaSuccess) e = dalloc(&a.perm2, cap);
   if (e == cudaSuccess) e = dalloc(&a.q_tmp, cap);
   if (e == cudaSuccess) e = dalloc(&a.v_tmp, cap);
+  if (e == cudaSuccess) e = dalloc(&a.v_lag, cap);
   if (e == cudaSuccess) e = dalloc(&a.ids_tmp, cap);
   if (e == cudaSuccess) e = dalloc(&a.type_tmp, cap);
   if (e == cudaSuccess) e = dalloc(&a.cell_tmp, cap);
@@ -992,6 +997,7 @@ mdg_status mdg_set_state(mdg_handle *h, const double *q4, const double *v4, cons
   st.error = 0;
   st.list_stale = 1;
   st.vmax2_bits = 0;
+  st.vlag_set = 0;
   st.budget = h->prm.buffer_length;
   CUDA_TRY(h, cudaMemcpyAsync(h->a.st, &st, sizeof(Status), cudaMemcpyHostToDevice, h->stream));
   if (n > 0) k_vmax<kBlock><<<blocks_for(n, kBlock), kBlock, 0, h->stream>>>(h->a, n);
@@ -1031,6 +1037,18 @@ mdg_status mdg_set_velocities(mdg_handle *h, const double *v4, int n) {
   if (n == 0) return MDG_OK;
   CUDA_TRY(h, cudaSetDevice(h->prm.device));
   h->fix_buf = -1;  // the fused step's packed first-drift copy used the old velocities
+  if (h->obs_lag > 0.0) {
+    // the reference's ghost copies date from half a step back: their
+    // reconstruction needs the velocities of the last drift, kept once
+    // (a second call before the next step keeps the first copy)
+    Status st;
+    if ((r = read_status(h, &st))) return r;
+    if (!st.vlag_set) {
+      const int one = 1;
+      CUDA_TRY(h, cudaMemcpyAsync(h->a.v_lag, h->a.v, sizeof(double4) * n, cudaMemcpyDeviceToDevice, h->stream));
+      CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->vlag_set, &one, sizeof one, cudaMemcpyHostToDevice, h->stream));
+    }
+  }
   const unsigned long long zero = 0ull;
   CUDA_TRY(h, cudaMemcpyAsync(h->a.v, v4, sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
   CUDA_TRY(h, cudaMemcpyAsync(&h->a.st->vmax2_bits, &zero, sizeof zero, cudaMemcpyHostToDevice, h->stream));
@@ -1587,6 +1605,7 @@ struct CkptHeader {
   External ext;
 };
 const char kCkptMagic[8] = {'M', 'D', 'G', 'C', 'K', 'P', 'T', '1'};
+constexpr int kCkptVersion = 2;  // 2: Status::vlag_set, and v_lag after the arrays when it is set
 }  // namespace
 
 mdg_status mdg_save_checkpoint(mdg_handle *h, const char *path) {
@@ -1596,7 +1615,7 @@ mdg_status mdg_save_checkpoint(mdg_handle *h, const char *path) {
   CUDA_TRY(h, cudaSetDevice(h->prm.device));
   CkptHeader hd{};
   memcpy(hd.magic, kCkptMagic, 8);
-  hd.version = 1;
+  hd.version = kCkptVersion;
   hd.n = h->n;
   for (int d = 0; d < 3; d++) hd.L[d] = h->prm.L[d];
   hd.cutoff = h->prm.cutoff;
@@ -1615,9 +1634,11 @@ mdg_status mdg_save_checkpoint(mdg_handle *h, const char *path) {
   if ((r = read_status(h, &hd.st))) return r;
   if (hd.st.error) return translate_device_error(h, hd.st);
   const int n = h->n;
-  std::vector<double4> q(n), v(n), qo(n);
+  std::vector<double4> q(n), v(n), qo(n), vl(hd.st.vlag_set ? n : 0);
   std::vector<int> ids(n), ty(n);
   if (n > 0) {
+    if (hd.st.vlag_set)
+      CUDA_TRY(h, cudaMemcpyAsync(vl.data(), h->a.v_lag, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(q.data(), h->a.q, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(v.data(), h->a.v, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(qo.data(), h->a.q_old, sizeof(double4) * n, cudaMemcpyDeviceToHost, h->stream));
@@ -1633,6 +1654,7 @@ mdg_status mdg_save_checkpoint(mdg_handle *h, const char *path) {
   f.write((const char *)qo.data(), sizeof(double4) * n);
   f.write((const char *)ids.data(), sizeof(int) * n);
   f.write((const char *)ty.data(), sizeof(int) * n);
+  f.write((const char *)vl.data(), sizeof(double4) * vl.size());
   if (!f) return fail(h, MDG_ERR_IO, std::string("write failed: ") + path);
   return MDG_OK;
 }
@@ -1643,7 +1665,7 @@ mdg_status mdg_load_checkpoint(mdg_handle *h, const char *path) {
   if (!f) return fail(h, MDG_ERR_IO, std::string("cannot read ") + path);
   CkptHeader hd{};
   f.read((char *)&hd, sizeof hd);
-  if (!f || memcmp(hd.magic, kCkptMagic, 8) != 0 || hd.version != 1 || hd.n < 0)
+  if (!f || memcmp(hd.magic, kCkptMagic, 8) != 0 || hd.version != kCkptVersion || hd.n < 0)
     return fail(h, MDG_ERR_IO, std::string("not a checkpoint of this library: ") + path);
   for (int d = 0; d < 3; d++)
     if (hd.L[d] != h->prm.L[d]) return fail(h, MDG_ERR_INVALID_ARGUMENT, "checkpoint box differs from the handle's");
@@ -1653,13 +1675,14 @@ mdg_status mdg_load_checkpoint(mdg_handle *h, const char *path) {
     return fail(h, MDG_ERR_INVALID_ARGUMENT, "checkpoint parameters differ from the handle's");
   const int n = hd.n;
   if (n > h->cap) return fail(h, MDG_ERR_CAPACITY, "checkpoint holds more atoms than the handle's capacity");
-  std::vector<double4> q(n), v(n), qo(n);
+  std::vector<double4> q(n), v(n), qo(n), vl(hd.st.vlag_set ? n : 0);
   std::vector<int> ids(n), ty(n);
   f.read((char *)q.data(), sizeof(double4) * n);
   f.read((char *)v.data(), sizeof(double4) * n);
   f.read((char *)qo.data(), sizeof(double4) * n);
   f.read((char *)ids.data(), sizeof(int) * n);
   f.read((char *)ty.data(), sizeof(int) * n);
+  f.read((char *)vl.data(), sizeof(double4) * vl.size());
   if (!f) return fail(h, MDG_ERR_IO, std::string("truncated checkpoint: ") + path);
   mdg_status r = mdg_set_control(h, hd.thermostat, hd.aimed_temperature, hd.heatbath_tau, hd.heatbath_gamma);
   if (r) return r;
@@ -1705,10 +1728,13 @@ mdg_status mdg_load_checkpoint(mdg_handle *h, const char *path) {
     st.max_row = built.max_row;
     st.list_entries = built.list_entries;
     st.total_images = built.total_images;
+    if (st.vlag_set)
+      CUDA_TRY(h, cudaMemcpyAsync(h->a.v_lag, vl.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(h->a.st, &st, sizeof(Status), cudaMemcpyHostToDevice, h->stream));
   } else {
     st = hd.st;
     st.list_stale = 1;
+    st.vlag_set = 0;  // the next step rebuilds: fresh ghost copies
     CUDA_TRY(h, cudaMemcpyAsync(h->a.st, &st, sizeof(Status), cudaMemcpyHostToDevice, h->stream));
   }
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));

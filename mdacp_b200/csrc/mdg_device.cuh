@@ -93,6 +93,12 @@ struct Status {
   double too_fast_v;                // speed that tripped kErrTooFast
   double ext_position;              // external executor: current piston position
   double ext_impulse;               // external executor: impulse of the last pass
+  // 1 while Arrays::v_lag holds the velocities of the last second half
+  // drift: an executor changed v after the step, and the reconstruction of
+  // the reference's half-step-old ghost copies (q - v dt/2) must use the
+  // velocities the drift used.  Cleared once the next step's skin check is
+  // decided, and by a rebuild (fresh copies).
+  int vlag_set;
 };
 
 // An executor the reference's projects run after every Calculate() (on the
@@ -121,6 +127,7 @@ struct Arrays {
   int *slot;          // rank inside the cell from the atomic scatter
   int *perm, *perm2;  // new slot -> old slot
   double4 *q_tmp, *v_tmp;
+  double4 *v_lag;     // velocities of the last second half drift (Status::vlag_set); null in slabs
   int *ids_tmp, *type_tmp, *cell_tmp;
   unsigned char *mult; // ghost-border membership at the last build (bits, see border_bits)
   int2 *cand;         // displacement-check candidates: (slot, image code)
@@ -266,12 +273,10 @@ __global__ void __launch_bounds__(BLOCK) k_vmax(Arrays a, int n) {
 
 // PairList::IsPairListExpired (src/pairlist.cc:25-65): budget -= 2 vmax dt
 // while the budget is positive (a too-fast atom is an error), then arm the
-// displacement check once the budget is spent.  Sets the two conditional
-// handles of this step's graph (or device flags in eager mode).
-static __global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_disp,
-                                cudaGraphConditionalHandle h_build, int in_graph, int *eager_flags) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  Status *st = a.st;
+// displacement check once the budget is spent.  One thread: *disp_out = run
+// the displacement check this step; returns whether the step rebuilds
+// unconditionally (a stale list).
+__device__ __forceinline__ int expiry_decide(Status *st, const Box &b, int *disp_out) {
   int disp = 0, build = 0;
   if (st->error == 0) {
     if (st->list_stale) {
@@ -297,6 +302,19 @@ static __global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_di
   }
   st->want_build = build;
   st->vmax2_bits = 0ull;
+  if (!disp) st->vlag_set = 0;  // no displacement check reads the ghost copies this step
+  *disp_out = disp;
+  return build;
+}
+
+// expiry_decide as a kernel: sets the two conditional handles of this
+// step's graph (or device flags in eager mode).
+static __global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_disp,
+                                cudaGraphConditionalHandle h_build, int in_graph, int *eager_flags) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Status *st = a.st;
+  int disp = 0;
+  const int build = expiry_decide(st, b, &disp);
   // the rebuild decision when no displacement check runs; otherwise k_decide,
   // after the check, sets it again
   const int build_now = st->error == 0 && build;
@@ -314,6 +332,7 @@ static __global__ void k_expiry(Arrays a, Box b, cudaGraphConditionalHandle h_di
 static __global__ void k_decide(Arrays a, cudaGraphConditionalHandle h_build, int in_graph, int *eager_flags) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int build = (a.st->error == 0) && a.st->want_build;
+  a.st->vlag_set = 0;  // the displacement check has read the ghost copies
   if (in_graph) cudaGraphSetConditional(h_build, build);
   else eager_flags[1] = build;
 }
@@ -393,7 +412,14 @@ __device__ __forceinline__ void for_each_copy(const CopyView &cv, const double L
       }
 }
 
-__device__ __forceinline__ CopyView copy_view(const Arrays &a) { return CopyView{a.q_old, a.q, a.v, a.mult}; }
+// Velocities that date the ghost copies: v_lag after an executor changed v.
+__device__ __forceinline__ const double4 *lag_velocities(const Arrays &a) {
+  return (a.v_lag && a.st->vlag_set) ? a.v_lag : a.v;
+}
+
+__device__ __forceinline__ CopyView copy_view(const Arrays &a) {
+  return CopyView{a.q_old, a.q, lag_velocities(a), a.mult};
+}
 
 // PairList::CheckByDisplacement, first pass: max |qb_old - q|^2 over all
 // copies (src/pairlist.cc:67-84).
@@ -440,6 +466,23 @@ struct PairStage {
 // an "any" over the pairs, so splitting the rows over blocks and the columns
 // over threads changes only the time.  l must be the same for every thread
 // of the block (the staging pass ends in a barrier).
+// The same reading the copies' positions from global memory (any l).
+template <int BLOCK>
+__device__ __forceinline__ void candidate_pair_test_global(const CopyView &cv, const double L[3], const int2 *cand,
+                                                           int l, double lag, double sl2, double rc2, int part,
+                                                           int parts, volatile int *found) {
+  for (int a = part; a < l - 1 && !*found; a += parts) {
+    double o1[3], n1[3];
+    copy_positions(cv, L, cand[a].x, cand[a].y, lag, o1, n1);
+    for (int c = a + 1 + threadIdx.x; c < l; c += BLOCK) {
+      double o2[3], n2[3];
+      copy_positions(cv, L, cand[c].x, cand[c].y, lag, o2, n2);
+      if (dist2(o1, o2) < sl2) continue;
+      if (dist2(n1, n2) < rc2) *found = 1;
+    }
+  }
+}
+
 template <int BLOCK>
 __device__ __forceinline__ void candidate_pair_test(const CopyView &cv, const double L[3], const int2 *cand, int l,
                                                     double lag, double sl2, double rc2, int part, int parts,
@@ -466,16 +509,7 @@ __device__ __forceinline__ void candidate_pair_test(const CopyView &cv, const do
       }
     }
   } else {
-    for (int a = part; a < l - 1 && !*found; a += parts) {
-      double o1[3], n1[3];
-      copy_positions(cv, L, cand[a].x, cand[a].y, lag, o1, n1);
-      for (int c = a + 1 + threadIdx.x; c < l; c += BLOCK) {
-        double o2[3], n2[3];
-        copy_positions(cv, L, cand[c].x, cand[c].y, lag, o2, n2);
-        if (dist2(o1, o2) < sl2) continue;
-        if (dist2(n1, n2) < rc2) *found = 1;
-      }
-    }
+    candidate_pair_test_global<BLOCK>(cv, L, cand, l, lag, sl2, rc2, part, parts, found);
   }
 }
 
@@ -884,12 +918,27 @@ __device__ __forceinline__ bool within_search_exact(const double4 &qi, const dou
   return !(r2 > sl2);
 }
 
+// Image shift of a stencil piece, 2 bits per axis (0: none, 1: -L, 2: +L).
+__device__ __forceinline__ double shift_of(int code, int d, const double L[3]) {
+  const int c = (code >> (2 * d)) & 3;
+  return c == 1 ? -L[d] : (c == 2 ? L[d] : 0.0);
+}
+
+// The exact test of candidate j of atom i through image shift `shift`
+// (within_search_exact).  Reached only for candidates in the FP32 band, so
+// the FP64 positions and shifts are read here rather than held in registers
+// across the candidate loop.
+__device__ __forceinline__ bool band_test(const double4 *__restrict__ q, int i, int j, int shift, const Box &b) {
+  return within_search_exact(q[i], q[j], shift_of(shift, 0, b.L), shift_of(shift, 1, b.L), shift_of(shift, 2, b.L),
+                             b.sl2);
+}
+
 // Candidates [beg, end) of one stencil row of atom i, in slot order: FP32
 // prefilter r^2 <= hi on the prefilter coordinates moved by the row's base
 // (bx, by, bz); the ghost-existence rule for image shifts (NEED); the exact
-// FP64 test for candidates in the band [lo, hi]; emit(j, k) files partner j
-// as entry k of the row.  SELF: the range holds atom i itself.  Four loads
-// are issued before the first test.
+// FP64 test for candidates in the band [lo, hi] (band_test, image shift
+// `shift`); emit(j, k) files partner j as entry k of the row.  SELF: the
+// range holds atom i itself.  Four loads are issued before the first test.
 //
 // With BTPA lanes per atom (the lanes of one atom are consecutive and all
 // walk the same ranges), lane s tests candidates beg + s, beg + BTPA + s, ...
@@ -899,16 +948,15 @@ __device__ __forceinline__ bool within_search_exact(const double4 &qi, const dou
 template <bool NEED, bool SELF, int BTPA, typename Emit>
 __device__ __forceinline__ void build_range(const float4 *__restrict__ qloc, const double4 *__restrict__ q,
                                             const unsigned char *__restrict__ mult, int beg, int end, float bx,
-                                            float by, float bz, int need, double sx, double sy, double sz, int i,
-                                            const double4 &qi, float lo, float hi, double sl2, int &cnt,
+                                            float by, float bz, int need, int shift, const Box &b, int i, int &cnt,
                                             Emit &emit) {
   auto keep_of = [&](int j, const float4 &l) {
     const float ex = l.x + bx, ey = l.y + by, ez = l.z + bz;
     const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-    bool keep = r2 <= hi;
+    bool keep = r2 <= b.sl2_hi;
     if (SELF) keep = keep && j != i;
     if (NEED) keep = keep && (mult[j] & need) == need;
-    if (keep && r2 >= lo) keep = within_search_exact(qi, q[j], sx, sy, sz, sl2);
+    if (keep && r2 >= b.sl2_lo) keep = band_test(q, i, j, shift, b);
     return keep;
   };
   if (BTPA == 1) {
@@ -966,27 +1014,34 @@ __device__ __forceinline__ int build_rows(const Box &b, const float4 *__restrict
                                           const double4 *__restrict__ q, const unsigned char *__restrict__ mult,
                                           const int *__restrict__ tab, int pc, int i, Emit &emit) {
   const float4 li = qloc[i];
-  const double4 qi = q[i];
   const int cx = pc & 2047, cy = (pc >> 11) & 2047, lz = pc >> 22;
   const int cz = SLAB ? b.z0 + lz : lz;  // global layer
   const int ms0 = b.ms[0], ms1 = b.ms[1], ms2 = b.ms[2];
-  const float lo = b.sl2_lo, hi = b.sl2_hi;
-  // sub-bins [vlo, vhi) of the virtual row of cells cx-1 .. cx+1 (unwrapped
-  // x) that can hold a partner: every bin that reaches [x_i - SL, x_i + SL]
-  const double cs0 = b.cs[0], per_bin = kXSub / cs0;
-  int vlo = (cx - 1) * kXSub + (int)floor((qi.x - (cx - 1) * cs0 - b.sl) * per_bin - 1e-6);
-  int vhi = (cx + 1) * kXSub + (int)floor((qi.x - (cx + 1) * cs0 + b.sl) * per_bin + 1e-6) + 1;
-  vlo = max(vlo, (cx - 1) * kXSub);
-  vhi = min(vhi, (cx + 2) * kXSub);
+  const float hi = b.sl2_hi;
   const int mx = ms0 * kXSub;
+  // sub-bins [vlo, vhi) of the virtual row of cells cx-1 .. cx+1 (unwrapped
+  // x) that can hold a partner: every bin that reaches [x_i - SL, x_i + SL];
+  // and the x bases of the three pieces (image shifts -L, 0, +L; prefilter
+  // x is global)
+  int vlo, vhi;
+  float bxm, bx0, bxp;
+  {
+    const double qx = q[i].x;
+    const double cs0 = b.cs[0], per_bin = kXSub / cs0;
+    vlo = (cx - 1) * kXSub + (int)floor((qx - (cx - 1) * cs0 - b.sl) * per_bin - 1e-6);
+    vhi = (cx + 1) * kXSub + (int)floor((qx - (cx + 1) * cs0 + b.sl) * per_bin + 1e-6) + 1;
+    vlo = max(vlo, (cx - 1) * kXSub);
+    vhi = min(vhi, (cx + 2) * kXSub);
+    bxm = (float)(-b.L[0] - qx);
+    bx0 = (float)(-qx);
+    bxp = (float)(b.L[0] - qx);
+  }
   const float csy = (float)b.cs[1], csz = (float)b.cs[2];
-  // x bases of the three pieces (image shifts -L, 0, +L); prefilter x is global
-  const float bxm = (float)(-b.L[0] - qi.x), bx0 = (float)(-qi.x), bxp = (float)(b.L[0] - qi.x);
   int cnt = 0;
   for (int dz = -1; dz <= 1; dz++) {
-    int z = cz + dz;
-    double sz = 0.0;
-    if (z < 0) { z += ms2; sz = -b.L[2]; } else if (z >= ms2) { z -= ms2; sz = b.L[2]; }
+    int z = cz + dz, zc = 0;  // zc: the row's image shift along z (shift_of's code)
+    if (z < 0) { z += ms2; zc = 1; } else if (z >= ms2) { z -= ms2; zc = 2; }
+    const double sz = zc == 1 ? -b.L[2] : (zc == 2 ? b.L[2] : 0.0);
     const float bz = (float)((z - cz) * b.cs[2] + sz) - li.z;
     const float gz = dz == 0 ? 0.f : (dz < 0 ? li.z : csz - li.z);
     // the layer's block of trim-table rows: the global layer in a single
@@ -999,41 +1054,41 @@ __device__ __forceinline__ int build_rows(const Box &b, const float4 *__restrict
     for (int dy = -1; dy <= 1; dy++) {
       const float gy = dy == 0 ? 0.f : (dy < 0 ? li.y : csy - li.y);
       if (fmaf(gy, gy, gz * gz) > hi) continue;  // the whole row is out of reach
-      int y = cy + dy;
-      double sy = 0.0;
-      if (y < 0) { y += ms1; sy = -b.L[1]; } else if (y >= ms1) { y -= ms1; sy = b.L[1]; }
+      int y = cy + dy, yc = 0;
+      if (y < 0) { y += ms1; yc = 1; } else if (y >= ms1) { y -= ms1; yc = 2; }
+      const double sy = yc == 1 ? -b.L[1] : (yc == 2 ? b.L[1] : 0.0);
       const float by = (float)((y - cy) * b.cs[1] + sy) - li.y;
       const int *xr = tab + (size_t)(blk * ms1 + y) * (mx + 1);
-      if (vlo < 0) {  // through the -x face: the row's last cells, image shift -L
-        const double sx = -b.L[0];
-        const int need = needed_strips(sx, sy, sz);
-        build_range<true, false, BTPA>(qloc, q, mult, xr[vlo + mx], xr[mx], bxm, by, bz, need, sx, sy, sz, i, qi, lo, hi,
-                                 b.sl2, cnt, emit);
-      }
+      const int yz = (yc << 2) | (zc << 4);
+      if (vlo < 0)  // through the -x face: the row's last cells, image shift -L
+        build_range<true, false, BTPA>(qloc, q, mult, xr[vlo + mx], xr[mx], bxm, by, bz,
+                                       needed_strips(-b.L[0], sy, sz), 1 | yz, b, i, cnt, emit);
       {
         const int a0 = max(vlo, 0), a1 = min(vhi, mx);
         const int beg = xr[a0], end = xr[a1];
         const int need = needed_strips(0.0, sy, sz);
         if (dz == 0 && dy == 0)
-          build_range<false, true, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, 0, 0.0, sy, sz, i, qi, lo, hi, b.sl2, cnt,
-                                   emit);
+          build_range<false, true, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, 0, yz, b, i, cnt, emit);
         else if (need)
-          build_range<true, false, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, need, 0.0, sy, sz, i, qi, lo, hi, b.sl2,
-                                   cnt, emit);
+          build_range<true, false, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, need, yz, b, i, cnt, emit);
         else
-          build_range<false, false, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, 0, 0.0, sy, sz, i, qi, lo, hi, b.sl2, cnt,
-                                    emit);
+          build_range<false, false, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, 0, yz, b, i, cnt, emit);
       }
-      if (vhi > mx) {  // through the +x face: the row's first cells, image shift +L
-        const double sx = b.L[0];
-        const int need = needed_strips(sx, sy, sz);
-        build_range<true, false, BTPA>(qloc, q, mult, xr[0], xr[vhi - mx], bxp, by, bz, need, sx, sy, sz, i, qi, lo, hi,
-                                 b.sl2, cnt, emit);
-      }
+      if (vhi > mx)  // through the +x face: the row's first cells, image shift +L
+        build_range<true, false, BTPA>(qloc, q, mult, xr[0], xr[vhi - mx], bxp, by, bz,
+                                       needed_strips(b.L[0], sy, sz), 2 | yz, b, i, cnt, emit);
     }
   }
   return cnt;
 }
+
+// Resident threads per SM the list build is compiled for (register cap
+// 65536 / this); the build is latency-bound, so occupancy is what hides its
+// load and branch latencies.
+#ifndef MDG_BUILD_THREADS_PER_SM
+#define MDG_BUILD_THREADS_PER_SM 0
+#endif
+constexpr int kBuildThreadsPerSM = MDG_BUILD_THREADS_PER_SM;
 
 // Stage offset of global slot j: the plan range whose atoms hold j (ranges
 // are sorted by first cell, so by first atom).
@@ -1054,7 +1109,8 @@ __device__ __forceinline__ int stage_shift_atom(const int4 *plan, int npl, int j
 // the pair set is the reference's bit for bit.  Rows are padded with the
 // atom's own index to a multiple of 4.
 template <int BLOCK, bool STAGE, bool SLAB = false, int BTPA = 1>
-__global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
+__global__ void __launch_bounds__(BLOCK, kBuildThreadsPerSM / BLOCK > 0 ? kBuildThreadsPerSM / BLOCK : 1)
+    k_build(Arrays a, Box b, int n) {
   static_assert(!(STAGE && SLAB), "staged rows are single-domain only");
   static_assert(!STAGE || BTPA == 1, "staged rows are built one lane per atom");
   const int t = blockIdx.x * BLOCK + threadIdx.x;
@@ -1147,6 +1203,7 @@ static __global__ void k_build_done(Arrays a, Box b) {
   if (st->error) return;
   st->budget = b.buffer_length;
   st->list_stale = 0;
+  st->vlag_set = 0;  // fresh ghost copies, and v_lag is in the old slot order
   st->rebuilds++;
 }
 
@@ -1187,7 +1244,10 @@ __device__ __forceinline__ double wall_df(double d, double c2, double dt) {
 // Before an executor pass: the pass re-takes the |v| maximum the next skin
 // check reads (PairList::IsPairListExpired reads the momenta after it).
 static __global__ void k_external_begin(Arrays a) {
-  if (threadIdx.x == 0 && blockIdx.x == 0 && !a.st->error) a.st->vmax2_bits = 0ull;
+  if (threadIdx.x == 0 && blockIdx.x == 0 && !a.st->error) {
+    a.st->vmax2_bits = 0ull;
+    if (a.v_lag) a.st->vlag_set = 1;  // k_external keeps the pre-pass velocities
+  }
 }
 
 // One executor pass over all atoms: GravityImposer (src/phaseflow.cc:58-73),
@@ -1200,6 +1260,7 @@ __global__ void __launch_bounds__(BLOCK) k_external(Arrays a, Box b, External x,
   if (i < n && !a.st->error) {
     const double4 q = a.q[i];
     double4 v = a.v[i];
+    if (a.v_lag) a.v_lag[i] = v;  // the velocities the step's second drift used
     const double CL = b.rc;
     if (x.kind == 1) {
       const double g = dmul(x.strength, x.dt);
@@ -1424,13 +1485,47 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // difference is the minimum-image displacement in units of L/2^32.  r^2 = 0
 // (the padding entries, the atom itself) contributes nothing: the unsigned
 // compare of the float bits keeps 0 < r^2 <= rc^2 in one test.
+#ifndef MDG_FP32_RCP
+#define MDG_FP32_RCP 0
+#endif
+#ifndef MDG_FP32_CVT
+#define MDG_FP32_CVT 0
+#endif
+__device__ __forceinline__ float rcp_newton(float x) {
+  float y = __int_as_float(0x7EF311C7 - __float_as_int(x));
+  float e = fmaf(-x, y, 1.f);
+  y = fmaf(y, e, y);
+  e = fmaf(-x, y, 1.f);
+  y = fmaf(y, e, y);
+  e = fmaf(-x, y, 1.f);
+  return fmaf(y, e, y);
+}
+__device__ __forceinline__ float i2f_split(int d) {
+  const float fhi = __int_as_float(0x4B400000 + (d >> 16)) - 12582912.0f;
+  const float flo = __int_as_float(0x4B000000 | ((unsigned)d & 0xFFFFu)) - 8388608.0f;
+  return fmaf(fhi, 65536.0f, flo);
+}
+__device__ __forceinline__ float cvt_f(int d) {
+#if MDG_FP32_CVT
+  return i2f_split(d);
+#else
+  return (float)d;
+#endif
+}
+__device__ __forceinline__ float rcp_f(float x) {
+#if MDG_FP32_RCP
+  return rcp_newton(x);
+#else
+  return rcp_approx(x);
+#endif
+}
 __device__ __forceinline__ void lj_pair_fp32(const int4 &pi, const int4 &pj, float sx, float sy, float sz,
                                              unsigned rc2_bits, float c2x8, float &fx, float &fy, float &fz) {
-  const float dx = (float)(pj.x - pi.x) * sx;
-  const float dy = (float)(pj.y - pi.y) * sy;
-  const float dz = (float)(pj.z - pi.z) * sz;
+  const float dx = cvt_f(pj.x - pi.x) * sx;
+  const float dy = cvt_f(pj.y - pi.y) * sy;
+  const float dz = cvt_f(pj.z - pi.z) * sz;
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float ir2 = rcp_approx(r2);
+  const float ir2 = rcp_f(r2);
   const float ir6 = ir2 * ir2 * ir2;
   float df = fmaf(ir2 * ir6, fmaf(-48.f, ir6, 24.f), c2x8);
   df = (__float_as_uint(r2) - 1u < rc2_bits) ? df : 0.f;
@@ -1475,20 +1570,23 @@ __device__ __forceinline__ void fp32_finish(Arrays &a, const Box &b, const Therm
 }
 
 // ------------------------------------------------ FP32 row sums, 1-4 lanes per atom
-// The row sum of an atom in a fixed order that does not depend on how many
-// lanes share the row, so that 1, 2 or 4 lanes per atom give bit-identical
-// forces: the row's G groups of four entries (rows are padded to a multiple
-// of 4 with masked self entries) are split into four quarters of
-// Q = ceil(G / 4) consecutive groups; inside a quarter the pair terms are
-// summed in FP32 over two groups (8 partners) at a time, in entry order, and
-// folded into the quarter's FP64 sum S_t; the row sum is
-// (S0 + S1) + (S2 + S3).  With TPA lanes per atom, lane s sums quarters
-// s*4/TPA .. (s+1)*4/TPA - 1 and the lanes combine by butterfly shuffles,
-// which form exactly that tree.
+// The row sum of an atom in one fixed order whatever the number of lanes
+// that share the row, so that 1, 2 or 4 lanes per atom give bit-identical
+// forces.  The row's G groups of four entries (rows are padded to a
+// multiple of 4 with masked self entries) form chunks of two groups (the
+// last chunk may hold one): chunk c is groups 2c and 2c + 1, its eight pair
+// terms summed in FP32 in entry order from 0; the row sum is the FP64 sum
+// of the chunk sums in chunk order, S = ((0 + s_0) + s_1) + ...  With TPA
+// lanes per atom, lane s sums chunks s, s + TPA, s + 2 TPA, ...; after each
+// round of TPA chunks every lane of the atom reads the round's chunk sums
+// from its neighbours (shuffles of FP32 values) and adds them in chunk
+// order, so every lane holds S at the end.  Chunks past the row's end add
+// +0.0, which leaves S unchanged (S starts at +0.0 and is never -0.0).
 
 // Partner positions of a lane's groups from the global fixed-point copy:
-// the four list entries of the next group are in flight while a group is
-// summed (the list is the one stream from HBM, so its loads run ahead).
+// the four list entries of the lane's next group are in flight while a
+// group is summed (the list is the one stream from HBM, so its loads run
+// ahead).  Group -1 is none: its entries are the atom itself.
 struct GlobalGroups {
   const int *row;  // nbr + atom
   int st;          // list stride
@@ -1496,18 +1594,24 @@ struct GlobalGroups {
   int self;
   int n0, n1, n2, n3, m0, m1, m2, m3;
   __device__ __forceinline__ void load(int g, int &x0, int &x1, int &x2, int &x3) const {
+    if (g < 0) {
+      x0 = x1 = x2 = x3 = self;
+      return;
+    }
     const int *r = row + (size_t)(4 * g) * st;
     x0 = __ldg(r);
     x1 = __ldg(r + st);
     x2 = __ldg(r + 2 * st);
     x3 = __ldg(r + 3 * st);
   }
-  __device__ __forceinline__ void start(int g, int gend) {
-    n0 = n1 = n2 = n3 = m0 = m1 = m2 = m3 = self;
-    if (g < gend) load(g, n0, n1, n2, n3);
-    if (g + 1 < gend) load(g + 1, m0, m1, m2, m3);
+  // the lane's first two groups
+  __device__ __forceinline__ void start(int ga, int gb) {
+    load(ga, n0, n1, n2, n3);
+    load(gb, m0, m1, m2, m3);
   }
-  __device__ __forceinline__ void take(int g, int gend, int4 &p0, int4 &p1, int4 &p2, int4 &p3) {
+  // positions of the lane's current group; the group after the next
+  // (gnext) starts loading
+  __device__ __forceinline__ void take(int gnext, int4 &p0, int4 &p1, int4 &p2, int4 &p3) {
     p0 = __ldg(qf + n0);
     p1 = __ldg(qf + n1);
     p2 = __ldg(qf + n2);
@@ -1516,13 +1620,13 @@ struct GlobalGroups {
     n1 = m1;
     n2 = m2;
     n3 = m3;
-    if (g + 2 < gend) load(g + 2, m0, m1, m2, m3);
+    load(gnext, m0, m1, m2, m3);
   }
 };
 
 // The same from the block's stage in shared memory: one 8-byte load brings
 // four 16-bit stage indices; indices outside the stage are flagged and read
-// as entry 0.
+// as entry 0.  One lane per atom.
 __device__ __forceinline__ unsigned stage_index(unsigned v, unsigned nstage, bool &bad) {
   const bool out = v >= nstage;
   bad |= out;
@@ -1536,19 +1640,21 @@ struct StagedGroups {
   unsigned nstage;
   bool bad;
   uint2 g0, g1;
-  __device__ __forceinline__ void start(int g, int gend) {
-    bad = false;
-    g0 = g1 = make_uint2(0u, 0u);
-    if (g < gend) g0 = __ldg(row + (size_t)g * st);
-    if (g + 1 < gend) g1 = __ldg(row + (size_t)(g + 1) * st);
+  __device__ __forceinline__ uint2 load(int g) const {
+    return g < 0 ? make_uint2(0u, 0u) : __ldg(row + (size_t)g * st);
   }
-  __device__ __forceinline__ void take(int g, int gend, int4 &p0, int4 &p1, int4 &p2, int4 &p3) {
+  __device__ __forceinline__ void start(int ga, int gb) {
+    bad = false;
+    g0 = load(ga);
+    g1 = load(gb);
+  }
+  __device__ __forceinline__ void take(int gnext, int4 &p0, int4 &p1, int4 &p2, int4 &p3) {
     p0 = pos[stage_index(g0.x & 0xffffu, nstage, bad)];
     p1 = pos[stage_index(g0.x >> 16, nstage, bad)];
     p2 = pos[stage_index(g0.y & 0xffffu, nstage, bad)];
     p3 = pos[stage_index(g0.y >> 16, nstage, bad)];
     g0 = g1;
-    if (g + 2 < gend) g1 = __ldg(row + (size_t)(g + 2) * st);
+    g1 = load(gnext);
   }
 };
 
@@ -1563,79 +1669,110 @@ __device__ __forceinline__ PairConst pair_const(const float fix_scale[3], float 
   return PairConst{fix_scale[0], fix_scale[1], fix_scale[2], __float_as_uint(rc2f), c2x8f};
 }
 
-// Lane `sub` (of TPA) of a row of G groups: its quarters' part of the sum
-// tree (see above); all TPA lanes must call, and after
-// combine_lanes<TPA> every lane of the atom holds the row sum.
+__device__ __forceinline__ void lj_group_fp32(const int4 &pi, const int4 &p0, const int4 &p1, const int4 &p2,
+                                              const int4 &p3, const PairConst &k, float &fx, float &fy, float &fz) {
+  lj_pair_fp32(pi, p0, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
+  lj_pair_fp32(pi, p1, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
+  lj_pair_fp32(pi, p2, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
+  lj_pair_fp32(pi, p3, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
+}
+
+// Row sum of an atom with G groups (see above), lane `sub` of TPA.  All TPA
+// lanes of the atom must call together (they exchange chunk sums); every
+// lane returns the row sum.
 template <int TPA, typename Groups>
-__device__ __forceinline__ void fp32_row_part(Groups &f, int G, int sub, const int4 &pi, const PairConst &k,
-                                              double &Fx, double &Fy, double &Fz) {
+__device__ __forceinline__ void fp32_row(Groups &f, int G, int sub, const int4 &pi, const PairConst &k, double &Fx,
+                                         double &Fy, double &Fz) {
   static_assert(TPA == 1 || TPA == 2 || TPA == 4, "1, 2 or 4 lanes per atom");
-  constexpr int QPL = 4 / TPA;  // quarters per lane
-  const int Q = (G + 3) >> 2;
-  const int q0 = sub * QPL;
-  const int gbeg = min(G, q0 * Q), gend = min(G, (q0 + QPL) * Q);
-  double Sx = 0.0, Sy = 0.0, Sz = 0.0, Px = 0.0, Py = 0.0, Pz = 0.0, Ax = 0.0, Ay = 0.0, Az = 0.0;
+  double Sx = 0.0, Sy = 0.0, Sz = 0.0;
   float fx = 0.f, fy = 0.f, fz = 0.f;
-  int qidx = q0, gq = 0;
-  auto close_quarter = [&]() {
-    if (TPA == 4 || (qidx & 1) == 0) {
-      Px = Sx; Py = Sy; Pz = Sz;
-    } else {
-      Px = Px + Sx; Py = Py + Sy; Pz = Pz + Sz;
-    }
-    if (TPA == 1 && qidx == 1) {
-      Ax = Px; Ay = Py; Az = Pz;
-    }
-    Sx = Sy = Sz = 0.0;
-    qidx++;
-  };
-  f.start(gbeg, gend);
-  for (int g = gbeg; g < gend; g++) {
-    int4 p0, p1, p2, p3;
-    f.take(g, gend, p0, p1, p2, p3);
-    lj_pair_fp32(pi, p0, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
-    lj_pair_fp32(pi, p1, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
-    lj_pair_fp32(pi, p2, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
-    lj_pair_fp32(pi, p3, k.sx, k.sy, k.sz, k.rc2_bits, k.c2x8, fx, fy, fz);
-    gq++;
-    const bool qend = gq == Q || g + 1 == gend;
-    if ((gq & 1) == 0 || qend) {
-      Sx += (double)fx;
-      Sy += (double)fy;
-      Sz += (double)fz;
-      fx = fy = fz = 0.f;
-    }
-    if (qend) {
-      close_quarter();
-      gq = 0;
-    }
-  }
-  while (qidx < q0 + QPL) close_quarter();  // quarters without groups: S_t = 0
   if (TPA == 1) {
-    Fx = Ax + Px; Fy = Ay + Py; Fz = Az + Pz;
+    f.start(G > 0 ? 0 : -1, G > 1 ? 1 : -1);
+    for (int g = 0; g < G; g++) {
+      int4 p0, p1, p2, p3;
+      f.take(g + 2 < G ? g + 2 : -1, p0, p1, p2, p3);
+      lj_group_fp32(pi, p0, p1, p2, p3, k, fx, fy, fz);
+      if (g & 1) {
+        Sx += (double)fx;
+        Sy += (double)fy;
+        Sz += (double)fz;
+        fx = fy = fz = 0.f;
+      }
+    }
+    Sx += (double)fx;  // the last chunk when it holds one group (else +0)
+    Sy += (double)fy;
+    Sz += (double)fz;
   } else {
-    Fx = Px; Fy = Py; Fz = Pz;
-  }
-}
-
-// Butterfly over the TPA lanes of an atom: lane pairs (0,1), (2,3) first,
-// then the two pairs -- the (S0 + S1) + (S2 + S3) tree (IEEE addition is
-// commutative, so both lanes of a pair hold the same value).  All lanes of
-// the warp must call.
-template <int TPA>
-__device__ __forceinline__ void combine_lanes(double &Fx, double &Fy, double &Fz) {
+    const int lane = threadIdx.x & 31;
+    const unsigned amask = ((1u << TPA) - 1u) << (lane & ~(TPA - 1));
+    const int C = (G + 1) >> 1, R = (C + TPA - 1) / TPA;
+    // the lane's m-th group: group 2c + (m & 1) of chunk c = sub + (m >> 1) TPA
+    auto grp = [&](int m) {
+      const int g = 2 * (sub + (m >> 1) * TPA) + (m & 1);
+      return g < G ? g : -1;
+    };
+    f.start(grp(0), grp(1));
+    for (int r = 0; r < R; r++) {
+      const int ga = grp(2 * r), gb = grp(2 * r + 1);
+      int4 p0, p1, p2, p3;
+      fx = fy = fz = 0.f;
+      f.take(grp(2 * r + 2), p0, p1, p2, p3);
+      if (ga >= 0) lj_group_fp32(pi, p0, p1, p2, p3, k, fx, fy, fz);
+      f.take(grp(2 * r + 3), p0, p1, p2, p3);
+      if (gb >= 0) lj_group_fp32(pi, p0, p1, p2, p3, k, fx, fy, fz);
 #pragma unroll
-  for (int o = 1; o < TPA; o <<= 1) {
-    Fx = Fx + __shfl_xor_sync(0xffffffffu, Fx, o);
-    Fy = Fy + __shfl_xor_sync(0xffffffffu, Fy, o);
-    Fz = Fz + __shfl_xor_sync(0xffffffffu, Fz, o);
+      for (int j = 0; j < TPA; j++) {
+        Sx += (double)__shfl_sync(amask, fx, j, TPA);
+        Sy += (double)__shfl_sync(amask, fy, j, TPA);
+        Sz += (double)__shfl_sync(amask, fz, j, TPA);
+      }
+    }
+  }
+  Fx = Sx;
+  Fy = Sy;
+  Fz = Sz;
+}
+
+// The error flag as one lane of the warp read it: the lanes of an atom must
+// agree on whether they take its row (they exchange values), and the flag
+// can be raised by another block at any time.  All lanes must call.
+__device__ __forceinline__ int warp_error(const Status *st) {
+  return __shfl_sync(0xffffffffu, *(volatile const int *)&st->error, 0);
+}
+
+// Sum of one value per atom over a block's BLOCK / TPA atoms (consecutive
+// atoms, TPA lanes each, the value on the atom's first lane), written to
+// partials[blockIdx.x].  The tree is block_sum_to<BLOCK / TPA, 1>'s over
+// one lane per atom whatever TPA is, so the sum does not depend on the lane
+// count.  All threads of the block must call.
+template <int BLOCK, int TPA>
+__device__ __forceinline__ void atom_block_sum(double x, double *partials) {
+  constexpr int ATOMS = BLOCK / TPA;
+  static_assert(ATOMS % 32 == 0, "whole warps of atoms");
+  __shared__ double per_atom[TPA > 1 ? ATOMS : 1];
+  __shared__ double per_warp[ATOMS / 32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (TPA > 1) {
+    if (threadIdx.x % TPA == 0) per_atom[threadIdx.x / TPA] = x;
+    __syncthreads();
+    x = threadIdx.x < ATOMS ? per_atom[threadIdx.x] : 0.0;
+  }
+  if (w < ATOMS / 32) {
+    const double s = warp_sum(x);
+    if (l == 0) per_warp[w] = s;
+  }
+  __syncthreads();
+  if (w == 0) {
+    double y = l < ATOMS / 32 ? per_warp[l] : 0.0;
+    y = warp_sum(y);
+    if (l == 0) partials[blockIdx.x] = y;
   }
 }
 
-// FP32-mixed force kick, TPA lanes per atom.  Displacements come from the
-// fixed-point copy (no ghost atoms, no shift codes); the row sum is
-// fp32_row_part's fixed-order tree and the kick is FP64 (lane 0 of the
-// atom).  With DRIFT the second half drift q += v dt/2 and the |v| maximum
+// FP32-mixed force kick, TPA lanes per atom (BLOCK / TPA atoms per block).
+// Displacements come from the fixed-point copy (no ghost atoms, no shift
+// codes); the row sum is fp32_row's fixed-order sum and the kick is FP64
+// (the atom's first lane).  With DRIFT the second half drift q += v dt/2 and the |v| maximum
 // of the step are done in the same pass: this kernel reads only the
 // fixed-point copy, so moving q here races with no other thread.  DRIFT == 2
 // is the whole NVE step in one pass: qf holds every atom's position after
@@ -1656,21 +1793,16 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Th
     a.st->steps++;
     a.st->sim_time += b.dt;
   }
-  const bool active = i < n && !a.st->error;
-  double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-  int4 pi = make_int4(0, 0, 0, 0);
-  if (active) {
-    pi = qf[i];
+  const int err = TPA > 1 ? warp_error(a.st) : a.st->error;
+  if (i < n && !err) {
+    const int4 pi = qf[i];
+    double Fx, Fy, Fz;
     GlobalGroups f{a.nbr + i, a.stride, qf, i};
-    fp32_row_part<TPA>(f, (a.nnbr[i] + 3) >> 2, sub, pi, pair_const(b.fix_scale, b.rc2f, b.c2x8f), Fx, Fy, Fz);
+    fp32_row<TPA>(f, (a.nnbr[i] + 3) >> 2, sub, pi, pair_const(b.fix_scale, b.rc2f, b.c2x8f), Fx, Fy, Fz);
+    if (sub == 0) fp32_finish<MODE, DRIFT>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
   }
-  combine_lanes<TPA>(Fx, Fy, Fz);
-  if (active && sub == 0) fp32_finish<MODE, DRIFT>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
   if (MODE == kKickLangevin || DRIFT) warp_max_to(&a.st->vmax2_bits, v2);
-  if (MODE == kKickNoseHoover) {
-    double s[1] = {ke};
-    block_sum_to<BLOCK, 1>(s, a.partials);
-  }
+  if (MODE == kKickNoseHoover) atom_block_sum<BLOCK, TPA>(ke, a.partials);
 }
 
 // ---------------------------------------------- mbarrier and bulk copies
@@ -1790,11 +1922,11 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32_staged(Arrays a, Box b, in
     double Fx = 0.0, Fy = 0.0, Fz = 0.0;
     if (use_stage) {
       StagedGroups f{a.nbr16 + i, a.stride, pos, nstage};
-      fp32_row_part<1>(f, G, 0, pi, k, Fx, Fy, Fz);
+      fp32_row<1>(f, G, 0, pi, k, Fx, Fy, Fz);
       if (f.bad) atomicOr(&a.st->error, kErrStage);
     } else {
       GlobalGroups f{a.nbr + i, a.stride, qf, i};
-      fp32_row_part<1>(f, G, 0, pi, k, Fx, Fy, Fz);
+      fp32_row<1>(f, G, 0, pi, k, Fx, Fy, Fz);
     }
     fp32_finish<MODE, DRIFT>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
   }
@@ -1860,61 +1992,123 @@ __device__ __forceinline__ bool take_step_alone(Status *st, const Box &b) {
   if (budget < 0.0) return false;
   st->budget = budget;
   st->vmax2_bits = 0ull;
+  st->vlag_set = 0;
   return true;
 }
 
 // Up to max_steps FP32-mixed NVE steps in one cooperative launch, for
 // systems small enough that per-step launch latency dominates: each step is
 // the fused pass of k_force_fp32<.., kKick, 2, TPA> over all atoms
-// (grid-stride), between two grid barriers -- one after the pass (every
-// position packed, the |v| maximum complete), one after block 0 has taken
-// the expiry decision.  The pass stops before the first step that needs the
-// displacement check or a rebuild, and before any error; out[0] returns the
-// steps taken, out[1] which fixed-point buffer holds the next step's
-// first-drift positions (0: qf0, 1: qf1).  The arithmetic is
-// k_force_fp32's, so trajectories equal the graph path's bit for bit.
+// (grid-stride), between grid barriers.  Block 0 takes the expiry decision
+// (take_step_alone, else expiry_decide); a step whose skin budget is spent
+// runs the displacement check of PairList::CheckByDisplacement in the same
+// launch, as k_disp_max, k_disp_collect and k_disp_pairs do it (copies
+// dated `lag` back), each phase ending in a grid barrier.  The pass stops
+// before the first step that needs a rebuild -- it marks the list stale, so
+// the caller's ordinary step rebuilds without deciding again -- and before
+// any error; out[0] returns the steps taken, out[1] which fixed-point buffer
+// holds the next step's first-drift positions (0: qf0, 1: qf1).  The
+// arithmetic is k_force_fp32's and the decisions are the graph path's, so
+// trajectories and counters equal the graph path's bit for bit.
 template <int BLOCK, int TPA>
 __global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n, int max_steps, int4 *qf0,
-                                                          int4 *qf1, int parity, GridBarrier *bar, int *out) {
+                                                          int4 *qf1, int parity, double lag, GridBarrier *bar,
+                                                          int *out) {
   __shared__ int go;
+  __shared__ volatile int found;
   const Thermo th{};
   const PairConst k = pair_const(b.fix_scale, b.rc2f, b.c2x8f);
   const long long nthreads = (long long)n * TPA;
   const long long stride = (long long)gridDim.x * BLOCK;
+  const int gtid = blockIdx.x * BLOCK + threadIdx.x, gthreads = gridDim.x * BLOCK;
+  Status *st = a.st;
+  volatile int *decision = &out[2];
   int steps = 0;
   for (; steps < max_steps; steps++) {
+    // 0: leave this step to the caller; 1: take it; 2: check displacements first
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-      const int g = take_step_alone(a.st, b) ? 1 : 0;
-      *(volatile int *)&out[2] = g;
-      if (g) {
-        a.st->steps++;
-        a.st->sim_time += b.dt;
+      int g = 0;
+      if (take_step_alone(st, b)) {
+        g = 1;
+      } else if (!st->error && !st->list_stale) {
+        int disp = 0;
+        expiry_decide(st, b, &disp);  // spends the budget; a too-fast atom is an error
+        g = st->error ? 0 : (disp ? 2 : 1);
       }
+      *decision = g;
       __threadfence();
     }
-    if (!grid_barrier(bar, a.st, kBarrierPolls)) break;
-    if (threadIdx.x == 0) go = *(volatile int *)&out[2];
+    if (!grid_barrier(bar, st, kBarrierPolls)) break;
+    if (threadIdx.x == 0) go = *decision;
     __syncthreads();
+    if (go == 2) {
+      double d2 = 0.0;
+      for (int i = gtid; i < n; i += gthreads)
+        for_each_copy(copy_view(a), b.L, i, lag, [&](int, double x) { d2 = fmax(d2, x); });
+      block_max_to<BLOCK>(&st->dr2max_bits, d2);
+      if (!grid_barrier(bar, st, kBarrierPolls)) break;
+      const double c = b.buffer_length - sqrt(__longlong_as_double(*(volatile long long *)&st->dr2max_bits));
+      const double c_d2 = c * c;
+      for (int i = gtid; i < n; i += gthreads)
+        for_each_copy(copy_view(a), b.L, i, lag, [&](int code, double x) {
+          if (x > c_d2) {
+            atomicAdd(&st->cand_weighted, 1);
+            const int kk = atomicAdd(&st->cand_n, 1);
+            if (kk < b.check_list_length) a.cand[kk] = make_int2(i, code);
+          }
+        });
+      if (!grid_barrier(bar, st, kBarrierPolls)) break;
+      if (threadIdx.x == 0) found = 0;
+      __syncthreads();
+      const long long tn = st->total_images;
+      const int nl = (int)((tn > b.check_list_length) ? b.check_list_length : tn);
+      const int weighted = *(volatile int *)&st->cand_weighted;
+      if (weighted >= nl) {
+        if (threadIdx.x == 0) found = 1;
+      } else {
+        const int l = min(*(volatile int *)&st->cand_n, b.check_list_length);
+        candidate_pair_test_global<BLOCK>(copy_view(a), b.L, a.cand, l, lag, b.sl2, b.rc2, blockIdx.x, gridDim.x,
+                                          &found);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0 && found) st->want_build = 1;
+      if (!grid_barrier(bar, st, kBarrierPolls)) break;
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // k_decide: a rebuild is left to the caller's ordinary step
+        const int build = !st->error && st->want_build;
+        st->vlag_set = 0;
+        if (build) st->list_stale = 1;
+        *decision = (build || st->error) ? 0 : 1;
+        __threadfence();
+      }
+      if (!grid_barrier(bar, st, kBarrierPolls)) break;
+      if (threadIdx.x == 0) go = *decision;
+      __syncthreads();
+    }
     if (!go) break;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->steps++;
+      st->sim_time += b.dt;
+    }
     const int4 *qf = parity ? qf1 : qf0;
     int4 *qf_next = parity ? qf0 : qf1;
     // warps walk whole warps of threads, so the lane shuffles stay converged
     for (long long base = (long long)blockIdx.x * BLOCK + (threadIdx.x & ~31); base < nthreads; base += stride) {
       const long long t = base + (threadIdx.x & 31);
       const int i = (int)(t / TPA), sub = (int)(t % TPA);
-      const bool active = t < nthreads && !a.st->error;
-      double Fx = 0.0, Fy = 0.0, Fz = 0.0, v2 = 0.0, ke = 0.0;
-      if (active) {
+      const int err = warp_error(st);
+      double v2 = 0.0, ke = 0.0;
+      if (t < nthreads && !err) {
         const int4 pi = qf[i];
+        double Fx, Fy, Fz;
         GlobalGroups f{a.nbr + i, a.stride, qf, i};
-        fp32_row_part<TPA>(f, (a.nnbr[i] + 3) >> 2, sub, pi, k, Fx, Fy, Fz);
+        fp32_row<TPA>(f, (a.nnbr[i] + 3) >> 2, sub, pi, k, Fx, Fy, Fz);
+        if (sub == 0) fp32_finish<kKick, 2>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
       }
-      combine_lanes<TPA>(Fx, Fy, Fz);
-      if (active && sub == 0) fp32_finish<kKick, 2>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
-      warp_max_to(&a.st->vmax2_bits, v2);
+      warp_max_to(&st->vmax2_bits, v2);
     }
     parity ^= 1;
-    if (!grid_barrier(bar, a.st, kBarrierPolls)) break;
+    if (!grid_barrier(bar, st, kBarrierPolls)) break;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     out[0] = steps;
@@ -1971,13 +2165,14 @@ __global__ void __launch_bounds__(BLOCK) k_observe(Arrays a, Box b, int n, doubl
     const double4 v = a.v[i];
     ke = dadd(dadd(dmul(dmul(0.5, v.x), v.x), dmul(dmul(0.5, v.y), v.y)), dmul(dmul(0.5, v.z), v.z));
     const double4 qi = a.q[i];
+    const double4 *vl = lag_velocities(a);
     const int nn = a.nnbr[i];
     for (int k = 0; k < nn; k++) {
       const int j = a.nbr[(size_t)k * a.stride + i];
       double4 qj = a.q[j];
       if (lag > 0.0 && (fabs(qj.x - qi.x) > b.hL[0] || fabs(qj.y - qi.y) > b.hL[1] ||
                         fabs(qj.z - qi.z) > b.hL[2])) {
-        const double4 vj = a.v[j];
+        const double4 vj = vl[j];
         qj.x = dsub(qj.x, dmul(vj.x, lag));
         qj.y = dsub(qj.y, dmul(vj.y, lag));
         qj.z = dsub(qj.z, dmul(vj.z, lag));

@@ -602,16 +602,16 @@ __global__ void __launch_bounds__(kEF) ke_force_fp32(Ens e) {
   const int i = t / TPA, sub = t % TPA;
   int r = 0;
   double v2 = 0.0;
-  const bool active = i < e.ntot && !*e.error;
+  // the lanes of an atom exchange chunk sums: they agree on the error flag
+  const int err = __shfl_sync(0xffffffffu, *(volatile const int *)e.error, 0);
+  const bool active = i < e.ntot && !err;
   double Fx = 0.0, Fy = 0.0, Fz = 0.0;
   if (active) {
     r = e.rep_of[i];
     const Rep &rep = e.rep[r];
     GlobalGroups f{e.nbr + i, e.stride, e.qfix, i};
-    fp32_row_part<TPA>(f, (e.nnbr[i] + 3) >> 2, sub, e.qfix[i], pair_const(rep.fix_scale, e.rc2f, e.c2x8f), Fx, Fy,
-                       Fz);
+    fp32_row<TPA>(f, (e.nnbr[i] + 3) >> 2, sub, e.qfix[i], pair_const(rep.fix_scale, e.rc2f, e.c2x8f), Fx, Fy, Fz);
   }
-  combine_lanes<TPA>(Fx, Fy, Fz);
   if (active && sub == 0) {
     const double dt = e.dt;
     double4 v = e.v[i];

@@ -66,7 +66,8 @@ class Variables {
   void QueueSteps(long n) { pending_steps += n; }
   // Runs queued steps, uploads host changes: after this the device is current.
   void SyncToDevice(void);
-  // Runs queued steps and downloads: after this the host arrays are current.
+  // Runs queued steps (uploading host changes first) and downloads: after
+  // this the host arrays are current.
   void SyncToHost(void);
 };
 // Aborts like the reference's show_error + exit(1) on a failed device call.

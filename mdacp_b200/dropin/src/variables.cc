@@ -187,7 +187,12 @@ void Variables::SyncToDevice(void) {
 
 void Variables::SyncToHost(void) {
   if (!device) return;
-  SyncToDevice();
+  // Host changes not yet uploaded leave the host arrays current: they go up
+  // before the next device step, not here (an executor that calls
+  // MDUnit::GetVariables several times would otherwise upload the whole
+  // state between its calls, which rebuilds the list and loses the ghost
+  // copies' age).  Queued steps run first, after the upload.
+  if (pending_steps > 0) SyncToDevice();
   if (device_newer) {
     mdg_check(device, mdg_get_state(device, &q[0][0], &p[0][0], type, particle_number), "mdg_get_state");
     mdg_check(device, mdg_get_zeta(device, &Zeta), "mdg_get_zeta");

@@ -8,6 +8,7 @@ import pytest
 
 import mdacp_b200 as M
 from mdacp_b200 import workloads as W
+from conftest import rankine_start
 from oracle import lj_oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -159,3 +160,74 @@ def test_host_kick_through_set_velocities_equals_device_gravity():
     assert np.array_equal(qa, qb) and np.array_equal(va, vb)
     ia, ib = a.info(), b.info()
     assert ia["rebuilds"] == ib["rebuilds"] and ia["displacement_checks"] == ib["displacement_checks"]
+
+
+
+def piston_kick(q, v, position, dt, cl=2.5):
+    """MyPiston::Execute (src/rankine.cc:66-97) on host arrays: the wall at
+    z = 0 and the piston at `position`; returns the new velocities and the
+    impulse (sequential sum)."""
+    s2 = 1.0 / (cl * cl)
+    s6 = s2 * s2 * s2
+    s8 = s6 * s2
+    s14 = s6 * s6 * s2
+    c2 = 6.0 * s14 - 3.0 * s8
+    v = v.copy()
+    imp = 0.0
+    for i in range(q.shape[0]):
+        z = q[i, 2]
+        if z < cl:
+            r2 = z * z
+            r6 = r2 * r2 * r2
+            df = ((24.0 * r6 - 48.0) / (r6 * r6 * r2) + c2 * 8.0) * dt
+            v[i, 2] -= df * z
+        if z > position:
+            dz = position - z + cl
+            r2 = dz * dz
+            r6 = r2 * r2 * r2
+            df = ((24.0 * r6 - 48.0) / (r6 * r6 * r2) + c2 * 8.0) * dt
+            v[i, 2] += df * dz
+            imp -= df * dz
+    return v, imp
+
+
+def test_rankine_piston_observers_match_oracle():
+    # the reference's Rankine loop from its start state (the oracle
+    # reproduces the project's printed rows): after every step the piston
+    # executor changes momenta -- on the device (mdg_set_external) and on the
+    # host, uploaded with set_velocities as the drop-in does -- and the
+    # observers see the reference's ghost copies, dated by the velocities of
+    # the step's drift, not the kicked ones
+    q, v, L = rankine_start()
+    n = q.shape[0]
+    dt, d_pos = 0.005, L[2] * 0.5 / 500
+    o = O.Oracle(q, v, np.arange(n, dtype=np.int32), L, 2.5, dt)
+    o.make_pairlist()
+    ox = O.External()
+    ox.kind, ox.position, ox.velocity, ox.time_step = M.EXTERNAL_PISTON, L[2] - 2.0, d_pos, dt
+    dev = M.System(L, cutoff=2.5, time_step=dt, capacity=n)
+    dev.set_state(q, v)
+    dev.set_external(kind=M.EXTERNAL_PISTON, position=L[2] - 2.0, velocity=d_pos, time_step=dt)
+    host = M.System(L, cutoff=2.5, time_step=dt, capacity=n)
+    host.set_state(q, v)
+    position = L[2] - 2.0
+    for s in (dev, host):
+        s.set_observer_mode(M.OBSERVE_GHOST_LAG)
+    q4, v4 = np.empty((n, 4)), np.empty((n, 4))
+    for i in range(151):
+        o.step(1)
+        o.apply_external(ox)
+        dev.calculate(1)
+        host.calculate(1)
+        host.get_state4(q4, v4)
+        v4[:, :3], _ = piston_kick(q4[:, :3], v4[:, :3], position, dt)
+        host.set_velocities4(v4)
+        position -= d_pos
+        if i % 50 == 0:
+            ref = o.observe()
+            for s in (dev, host):
+                got = s.observe()
+                for k in range(3):
+                    assert got[k] == pytest.approx(ref[k], rel=1e-10), (i, k)
+    assert dev.external_state()[0] == ox.position
+    o.close()

@@ -43,6 +43,23 @@ def test_lanes_and_blocks_bit_identical(rho):
         assert np.array_equal(q, states[0][0]) and np.array_equal(v, states[0][1])
 
 
+@pytest.mark.parametrize("thermostat", ["nose_hoover", "langevin"])
+def test_lanes_bit_identical_with_thermostats(thermostat):
+    # the Nose-Hoover kinetic energy partials cover the same atoms in the
+    # same tree whatever the lane count, and Langevin's noise is per atom
+    st = W.fcc_liquid(8, 0.8442, 1.0, seed=73, jitter=0.06, rc=2.5, dt=0.005)
+    kw = dict(thermostat=M.NOSE_HOOVER if thermostat == "nose_hoover" else M.LANGEVIN,
+              aimed_temperature=0.8, seed=9)
+    states = []
+    for tpa in (1, 2, 4):
+        s = _system(st, threads_per_atom=tpa, build_block=128, build_threads_per_atom=1, **kw)
+        s.calculate(60)
+        states.append(s.state_by_id())
+        s.close()
+    for q, v in states[1:]:
+        assert np.array_equal(q, states[0][0]) and np.array_equal(v, states[0][1])
+
+
 def test_autotune_picks_a_shape_and_keeps_the_trajectory():
     st = W.fcc_liquid(10, 0.8442, 0.9, seed=72, jitter=0.05, rc=2.5, dt=0.004)
     a = _system(st)                                    # tuned at the first step

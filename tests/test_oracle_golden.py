@@ -6,7 +6,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from conftest import pair_set
+from conftest import GOLDEN, pair_set
 from oracle import lj_oracle as O
 
 
@@ -59,3 +59,37 @@ def test_trajectory_bit_exact(golden):
     assert np.array_equal(qo, golden["traj_q"])
     assert np.array_equal(vo, golden["traj_v"])
     assert o.constructions == int(golden["constructions"])
+
+
+def rankine_rows(count):
+    """The oracle running the reference's Rankine loop (src/rankine.cc:101-128:
+    Calculate, the piston executor, the piston's move, observation every 50
+    steps) from the project's start state; rows as the project prints them."""
+    from conftest import rankine_start
+    q, v, L = rankine_start()
+    n = q.shape[0]
+    o = O.Oracle(q, v, np.arange(n, dtype=np.int32), L, 2.5, 0.005)
+    o.make_pairlist()
+    ox = O.External()
+    ox.kind, ox.position, ox.velocity, ox.time_step = 2, L[2] - 2.0, L[2] * 0.5 / 500, 0.005
+    rows = []
+    for i in range(50 * (count - 1) + 1):
+        o.step(1)
+        imp = o.apply_external(ox)
+        if i % 50 == 0:
+            ke, pe, vir = o.observe()
+            t = ke / n / 1.5
+            rows.append([(i + 1) * 0.005, t, (t - vir / n) * n / L.prod(), ke / n + pe / n, ox.position, imp])
+    o.close()
+    return rows
+
+
+def test_oracle_reproduces_reference_rankine_rows():
+    # the reference's own output for its Rankine project (piston executor
+    # after every step, observers on ghost copies half a step old), compared
+    # at the precision it prints: pins the executor and the ghost-lag
+    # observers of the oracle to the reference
+    text = (GOLDEN / "dropin_rankine_rc25.ref.txt").read_text().splitlines()
+    ref = [l.split("#")[0].split() for l in text if "#observe" in l][:4]
+    got = [["%g" % x for x in row] for row in rankine_rows(4)]
+    assert got == ref
