@@ -87,6 +87,8 @@ struct mdg_handle {
   bool state_set = false;
   // graph of kStepsPerGraph steps
   cudaGraphExec_t exec = nullptr;
+  cudaGraphExec_t rebuild_exec = nullptr;  // persistent pipeline: the guarded rebuild step
+  bool rebuild_dirty = true;
   bool graph_dirty = true;
   bool timing = false;
   bool use_graphs = true;
@@ -105,8 +107,10 @@ struct mdg_handle {
   int build_block = 0;                // threads per block of the list build (0: to be tuned)
   int build_tpa = 0;                  // lanes per atom of the list build (0: to be tuned)
   GridBarrier *d_bar = nullptr;       // persistent pass: grid barrier
-  int *d_pout = nullptr;              // persistent pass: steps taken, buffer parity, decision
+  int *d_pout = nullptr;              // persistent pass: block 0's decisions
   int64_t persistent_steps = 0;
+  int persist_grid = -1;              // blocks of the persistent pass (-1: not computed yet)
+  double steps_per_cycle = 4.0;       // persistent pipeline: steps per queued launch pair, as last seen
   External ext{};                     // executor applied after every step (kind 0: none)
   // snapshots: one set of pinned buffers per handle, at most one pending writer
   std::thread writer;
@@ -150,6 +154,10 @@ void free_arrays(Arrays &a) {
 void destroy_graph(mdg_handle *h) {
   if (h->exec) cudaGraphExecDestroy(h->exec);
   h->exec = nullptr;
+  if (h->rebuild_exec) cudaGraphExecDestroy(h->rebuild_exec);
+  h->rebuild_exec = nullptr;
+  h->rebuild_dirty = true;
+  h->persist_grid = -1;  // lanes per atom or the atom count may have changed
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   h->ev.clear();
   h->graph_dirty = true;
@@ -747,7 +755,7 @@ mdg_status autotune(mdg_handle *h) {
 // lanes, at most what the device keeps resident at once (a cooperative
 // launch needs all of them resident); 0 if the kernel cannot be resident.
 template <int TPA>
-int persistent_grid(mdg_handle *h) {
+int persistent_grid_of(mdg_handle *h) {
   int per_sm = 0, sms = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nve_persistent<kForceBlock, TPA>, kForceBlock, 0) !=
           cudaSuccess ||
@@ -757,36 +765,109 @@ int persistent_grid(mdg_handle *h) {
   return (int)std::min<long long>(need, (long long)per_sm * sms);
 }
 
+int persistent_grid(mdg_handle *h) {
+  if (h->persist_grid < 0) {
+    const int tpa = h->tpa > 0 ? h->tpa : 1;
+    h->persist_grid = tpa == 4 ? persistent_grid_of<4>(h) : (tpa == 2 ? persistent_grid_of<2>(h) : persistent_grid_of<1>(h));
+  }
+  return h->persist_grid;
+}
+
 // Whether mdg_calculate runs the persistent pass: asked for, or (auto) when
 // one wave of resident blocks covers every atom's lanes.
 bool use_persistent(mdg_handle *h) {
   if (!fused_step(h) || h->prm.step_mode == MDG_STEPS_GRAPHS) return false;
   const int tpa = h->tpa > 0 ? h->tpa : 1;
-  const int g = tpa == 4 ? persistent_grid<4>(h) : (tpa == 2 ? persistent_grid<2>(h) : persistent_grid<1>(h));
+  const int g = persistent_grid(h);
   if (g <= 0) return false;
   if (h->prm.step_mode == MDG_STEPS_PERSISTENT) return true;
   return (long long)g * kForceBlock >= (long long)h->n * tpa;
 }
 
-// Up to `steps` steps in one cooperative launch; *taken returns how many ran.
+// One persistent launch, queued (no wait): it takes steps until one needs a
+// rebuild or the step count reaches Status::target_steps.
 template <int TPA>
-mdg_status launch_persistent(mdg_handle *h, int steps, int *taken) {
-  const int grid = persistent_grid<TPA>(h);
+mdg_status enqueue_persistent_tpa(mdg_handle *h) {
+  const int grid = persistent_grid(h);
   if (grid <= 0) return fail(h, MDG_ERR_CUDA, "persistent pass: no resident grid");
   CUDA_TRY(h, cudaMemsetAsync(h->d_bar, 0, sizeof(GridBarrier), h->stream));
-  int n = h->n, parity = h->fix_buf > 0 ? 1 : 0;
+  int n = h->n;
   int4 *q0 = h->a.qfix, *q1 = h->a.qfix2;
   double lag = step_lag(h);  // the ghost copies' age at a step's displacement check
-  void *args[] = {&h->a, &h->box, &n, &steps, &q0, &q1, &parity, &lag, &h->d_bar, &h->d_pout};
+  void *args[] = {&h->a, &h->box, &n, &q0, &q1, &lag, &h->d_bar, &h->d_pout};
   CUDA_TRY(h, cudaLaunchCooperativeKernel((const void *)k_nve_persistent<kForceBlock, TPA>, dim3(grid),
                                           dim3(kForceBlock), args, 0, h->stream));
-  int out[2] = {0, 0};
-  CUDA_TRY(h, cudaMemcpyAsync(out, h->d_pout, sizeof out, cudaMemcpyDeviceToHost, h->stream));
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   h->kernel_launches++;
-  h->fix_buf = out[1];
-  *taken = out[0];
-  h->persistent_steps += out[0];
+  return MDG_OK;
+}
+
+mdg_status enqueue_persistent(mdg_handle *h) {
+  const int tpa = h->tpa > 0 ? h->tpa : 1;
+  return tpa == 4 ? enqueue_persistent_tpa<4>(h) : (tpa == 2 ? enqueue_persistent_tpa<2>(h) : enqueue_persistent_tpa<1>(h));
+}
+
+// The guarded rebuild step of the persistent pipeline (k_rebuild_guard):
+// rebuild with buffer 0 packed, the fused step from buffer 0, parity 1.
+mdg_status build_rebuild_graph(mdg_handle *h) {
+  if (h->rebuild_exec) cudaGraphExecDestroy(h->rebuild_exec);
+  h->rebuild_exec = nullptr;
+  cudaGraph_t g;
+  CUDA_TRY(h, cudaGraphCreate(&g, 0));
+  Capture c{h->cap_stream, g, {}};
+  cudaGraphConditionalHandle hr;
+  CUDA_TRY(h, cudaGraphConditionalHandleCreate(&hr, g, 0, cudaGraphCondAssignDefault));
+  CUDA_TRY(h, begin_capture(c));
+  k_rebuild_guard<<<1, 32, 0, c.s>>>(h->a, h->box, hr);
+  CUDA_TRY(h, end_capture(c));
+  cudaGraph_t body;
+  CUDA_TRY(h, add_if(c, hr, &body));
+  {
+    Capture bc{h->cap_stream, body, {}};
+    CUDA_TRY(h, begin_capture(bc));
+    launch_build(h, bc.s, h->a.qfix);
+    launch_force_mode<kKick>(h, bc.s, thermo_of(h), 2, h->a.qfix, h->a.qfix2);
+    k_set_parity<<<1, 32, 0, bc.s>>>(h->a, 1);
+    CUDA_TRY(h, end_capture(bc));
+  }
+  cudaError_t e = cudaGraphInstantiate(&h->rebuild_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(h, MDG_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  h->rebuild_dirty = false;
+  return MDG_OK;
+}
+
+// Steps up to `target` through the persistent pipeline: pairs of (persistent
+// launch, rebuild step) queued back to back without waiting -- each launch
+// stops where a step needs a rebuild, the rebuild step takes that step, and
+// both stop at the target, so queued pairs beyond it do nothing -- then one
+// wait and a status read per batch of pairs.  *st returns the final status.
+mdg_status run_persistent(mdg_handle *h, long long target, Status *st) {
+  mdg_status r;
+  if (h->fix_buf < 0) {
+    k_pack_half<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n, h->a.qfix);
+    h->kernel_launches++;
+    h->fix_buf = 0;
+  }
+  if (h->rebuild_dirty || !h->rebuild_exec) {
+    if ((r = build_rebuild_graph(h))) return r;
+  }
+  k_set_target<<<1, 32, 0, h->stream>>>(h->a, target, h->fix_buf > 0 ? 1 : 0);
+  long long steps = st->steps;
+  while (steps < target) {
+    const long long left = target - steps;
+    const int pairs = (int)std::min<long long>(64, (long long)std::ceil(left / h->steps_per_cycle) + 1);
+    for (int k = 0; k < pairs; k++) {
+      if ((r = enqueue_persistent(h))) return r;
+      CUDA_TRY(h, cudaGraphLaunch(h->rebuild_exec, h->stream));
+      h->kernel_launches += 2;
+    }
+    if ((r = read_status(h, st))) return r;
+    if (st->steps > steps) h->steps_per_cycle = std::max(1.0, (double)(st->steps - steps) / pairs);
+    if (st->error || st->steps == steps) break;
+    steps = st->steps;
+  }
+  h->fix_buf = st->fix_parity;
+  h->persistent_steps = st->persistent_steps;
   return MDG_OK;
 }
 
@@ -1002,7 +1083,10 @@ mdg_status mdg_set_state(mdg_handle *h, const double *q4, const double *v4, cons
   CUDA_TRY(h, cudaMemcpyAsync(h->a.st, &st, sizeof(Status), cudaMemcpyHostToDevice, h->stream));
   if (n > 0) k_vmax<kBlock><<<blocks_for(n, kBlock), kBlock, 0, h->stream>>>(h->a, n);
   CUDA_TRY(h, cudaGetLastError());
-  if (n != h->n) h->graph_dirty = true;
+  if (n != h->n) {
+    h->graph_dirty = h->rebuild_dirty = true;
+    h->persist_grid = -1;
+  }
   h->n = n;
   h->obs_lag = 0.0;
   int dev_error = 0;
@@ -1359,31 +1443,8 @@ mdg_status mdg_calculate(mdg_handle *h, int nsteps) {
       h->fix_buf = 0;
     }
     if (h->use_graphs && use_persistent(h)) {
-      // steps back to back in one launch until one needs the displacement
-      // check or a rebuild; that step runs as an ordinary step
-      while (left > 0) {
-        if (h->fix_buf < 0) {
-          k_pack_half<kBlock><<<blocks_for(h->n, kBlock), kBlock, 0, h->stream>>>(h->a, h->box, h->n, h->a.qfix);
-          h->kernel_launches++;
-          h->fix_buf = 0;
-        }
-        int taken = 0;
-        const int want = (int)std::min<long long>(left, 1 << 30);
-        const int tpa = h->tpa > 0 ? h->tpa : 1;
-        if ((r = tpa == 4 ? launch_persistent<4>(h, want, &taken)
-                          : (tpa == 2 ? launch_persistent<2>(h, want, &taken) : launch_persistent<1>(h, want, &taken))))
-          return r;
-        left -= taken;
-        if (left > 0) {
-          if ((r = step_eager(h))) return r;
-          left--;
-        }
-        if ((r = read_status(h, &st))) return r;
-        if (st.error) {
-          left = 0;  // handled below (a row overflow grows the rows and redoes the rest)
-          break;
-        }
-      }
+      if ((r = run_persistent(h, target, &st))) return r;
+      left = st.error ? 0 : target - st.steps;  // an error is handled below
     }
     if (h->use_graphs && left >= kStepsPerGraph && h->graph_dirty) {
       if ((r = build_graph(h))) return r;
@@ -1713,7 +1774,10 @@ mdg_status mdg_load_checkpoint(mdg_handle *h, const char *path) {
   st.error = 0;
   st.list_stale = 1;
   CUDA_TRY(h, cudaMemcpyAsync(h->a.st, &st, sizeof(Status), cudaMemcpyHostToDevice, h->stream));
-  if (n != h->n) h->graph_dirty = true;
+  if (n != h->n) {
+    h->graph_dirty = h->rebuild_dirty = true;
+    h->persist_grid = -1;
+  }
   h->n = n;
   h->state_set = true;
   h->fix_buf = -1;

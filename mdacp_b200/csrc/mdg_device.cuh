@@ -99,6 +99,13 @@ struct Status {
   // velocities the drift used.  Cleared once the next step's skin check is
   // decided, and by a rebuild (fresh copies).
   int vlag_set;
+  // persistent pipeline (mdg_calculate with the persistent pass): the step
+  // count the queued launches stop at, the fixed-point buffer the next
+  // fused step reads (0: qfix, 1: qfix2), and the steps the persistent
+  // pass took
+  long long target_steps;
+  int fix_parity;
+  long long persistent_steps;
 };
 
 // An executor the reference's projects run after every Calculate() (on the
@@ -1082,14 +1089,6 @@ __device__ __forceinline__ int build_rows(const Box &b, const float4 *__restrict
   return cnt;
 }
 
-// Resident threads per SM the list build is compiled for (register cap
-// 65536 / this); the build is latency-bound, so occupancy is what hides its
-// load and branch latencies.
-#ifndef MDG_BUILD_THREADS_PER_SM
-#define MDG_BUILD_THREADS_PER_SM 0
-#endif
-constexpr int kBuildThreadsPerSM = MDG_BUILD_THREADS_PER_SM;
-
 // Stage offset of global slot j: the plan range whose atoms hold j (ranges
 // are sorted by first cell, so by first atom).
 __device__ __forceinline__ int stage_shift_atom(const int4 *plan, int npl, int j) {
@@ -1109,8 +1108,7 @@ __device__ __forceinline__ int stage_shift_atom(const int4 *plan, int npl, int j
 // the pair set is the reference's bit for bit.  Rows are padded with the
 // atom's own index to a multiple of 4.
 template <int BLOCK, bool STAGE, bool SLAB = false, int BTPA = 1>
-__global__ void __launch_bounds__(BLOCK, kBuildThreadsPerSM / BLOCK > 0 ? kBuildThreadsPerSM / BLOCK : 1)
-    k_build(Arrays a, Box b, int n) {
+__global__ void __launch_bounds__(BLOCK) k_build(Arrays a, Box b, int n) {
   static_assert(!(STAGE && SLAB), "staged rows are single-domain only");
   static_assert(!STAGE || BTPA == 1, "staged rows are built one lane per atom");
   const int t = blockIdx.x * BLOCK + threadIdx.x;
@@ -1485,47 +1483,13 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // difference is the minimum-image displacement in units of L/2^32.  r^2 = 0
 // (the padding entries, the atom itself) contributes nothing: the unsigned
 // compare of the float bits keeps 0 < r^2 <= rc^2 in one test.
-#ifndef MDG_FP32_RCP
-#define MDG_FP32_RCP 0
-#endif
-#ifndef MDG_FP32_CVT
-#define MDG_FP32_CVT 0
-#endif
-__device__ __forceinline__ float rcp_newton(float x) {
-  float y = __int_as_float(0x7EF311C7 - __float_as_int(x));
-  float e = fmaf(-x, y, 1.f);
-  y = fmaf(y, e, y);
-  e = fmaf(-x, y, 1.f);
-  y = fmaf(y, e, y);
-  e = fmaf(-x, y, 1.f);
-  return fmaf(y, e, y);
-}
-__device__ __forceinline__ float i2f_split(int d) {
-  const float fhi = __int_as_float(0x4B400000 + (d >> 16)) - 12582912.0f;
-  const float flo = __int_as_float(0x4B000000 | ((unsigned)d & 0xFFFFu)) - 8388608.0f;
-  return fmaf(fhi, 65536.0f, flo);
-}
-__device__ __forceinline__ float cvt_f(int d) {
-#if MDG_FP32_CVT
-  return i2f_split(d);
-#else
-  return (float)d;
-#endif
-}
-__device__ __forceinline__ float rcp_f(float x) {
-#if MDG_FP32_RCP
-  return rcp_newton(x);
-#else
-  return rcp_approx(x);
-#endif
-}
 __device__ __forceinline__ void lj_pair_fp32(const int4 &pi, const int4 &pj, float sx, float sy, float sz,
                                              unsigned rc2_bits, float c2x8, float &fx, float &fy, float &fz) {
-  const float dx = cvt_f(pj.x - pi.x) * sx;
-  const float dy = cvt_f(pj.y - pi.y) * sy;
-  const float dz = cvt_f(pj.z - pi.z) * sz;
+  const float dx = (float)(pj.x - pi.x) * sx;
+  const float dy = (float)(pj.y - pi.y) * sy;
+  const float dz = (float)(pj.z - pi.z) * sz;
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float ir2 = rcp_f(r2);
+  const float ir2 = rcp_approx(r2);
   const float ir6 = ir2 * ir2 * ir2;
   float df = fmaf(ir2 * ir6, fmaf(-48.f, ir6, 24.f), c2x8);
   df = (__float_as_uint(r2) - 1u < rc2_bits) ? df : 0.f;
@@ -1583,16 +1547,18 @@ __device__ __forceinline__ void fp32_finish(Arrays &a, const Box &b, const Therm
 // order, so every lane holds S at the end.  Chunks past the row's end add
 // +0.0, which leaves S unchanged (S starts at +0.0 and is never -0.0).
 
-// Partner positions of a lane's groups from the global fixed-point copy:
-// the four list entries of the lane's next group are in flight while a
-// group is summed (the list is the one stream from HBM, so its loads run
-// ahead).  Group -1 is none: its entries are the atom itself.
+// Partner positions of a lane's groups from the global fixed-point copy,
+// software-pipelined: while a group is summed, the next group's positions
+// and the list entries of the group after it are in flight (the gathers
+// are the pass's long-latency loads, the list its one stream from HBM).
+// Group -1 is none: its entries are the atom itself.
 struct GlobalGroups {
   const int *row;  // nbr + atom
   int st;          // list stride
   const int4 *qf;
   int self;
-  int n0, n1, n2, n3, m0, m1, m2, m3;
+  int m0, m1, m2, m3;      // entries of the next group
+  int4 c0, c1, c2, c3;     // positions of the current group
   __device__ __forceinline__ void load(int g, int &x0, int &x1, int &x2, int &x3) const {
     if (g < 0) {
       x0 = x1 = x2 = x3 = self;
@@ -1606,20 +1572,25 @@ struct GlobalGroups {
   }
   // the lane's first two groups
   __device__ __forceinline__ void start(int ga, int gb) {
+    int n0, n1, n2, n3;
     load(ga, n0, n1, n2, n3);
+    c0 = __ldg(qf + n0);
+    c1 = __ldg(qf + n1);
+    c2 = __ldg(qf + n2);
+    c3 = __ldg(qf + n3);
     load(gb, m0, m1, m2, m3);
   }
-  // positions of the lane's current group; the group after the next
-  // (gnext) starts loading
+  // positions of the lane's current group; the next group's positions and
+  // the entries of the group after it (gnext) start loading
   __device__ __forceinline__ void take(int gnext, int4 &p0, int4 &p1, int4 &p2, int4 &p3) {
-    p0 = __ldg(qf + n0);
-    p1 = __ldg(qf + n1);
-    p2 = __ldg(qf + n2);
-    p3 = __ldg(qf + n3);
-    n0 = m0;
-    n1 = m1;
-    n2 = m2;
-    n3 = m3;
+    p0 = c0;
+    p1 = c1;
+    p2 = c2;
+    p3 = c3;
+    c0 = __ldg(qf + m0);
+    c1 = __ldg(qf + m1);
+    c2 = __ldg(qf + m2);
+    c3 = __ldg(qf + m3);
     load(gnext, m0, m1, m2, m3);
   }
 };
@@ -1996,7 +1967,7 @@ __device__ __forceinline__ bool take_step_alone(Status *st, const Box &b) {
   return true;
 }
 
-// Up to max_steps FP32-mixed NVE steps in one cooperative launch, for
+// FP32-mixed NVE steps in one cooperative launch, for
 // systems small enough that per-step launch latency dominates: each step is
 // the fused pass of k_force_fp32<.., kKick, 2, TPA> over all atoms
 // (grid-stride), between grid barriers.  Block 0 takes the expiry decision
@@ -2006,14 +1977,15 @@ __device__ __forceinline__ bool take_step_alone(Status *st, const Box &b) {
 // dated `lag` back), each phase ending in a grid barrier.  The pass stops
 // before the first step that needs a rebuild -- it marks the list stale, so
 // the caller's ordinary step rebuilds without deciding again -- and before
-// any error; out[0] returns the steps taken, out[1] which fixed-point buffer
-// holds the next step's first-drift positions (0: qf0, 1: qf1).  The
-// arithmetic is k_force_fp32's and the decisions are the graph path's, so
-// trajectories and counters equal the graph path's bit for bit.
+// any error, or when the step count reaches Status::target_steps.  The
+// fixed-point buffer the next step reads comes from, and goes back to,
+// Status::fix_parity (0: qf0, 1: qf1); out[0] broadcasts block 0's
+// decisions.  The arithmetic is k_force_fp32's and the decisions are the
+// graph path's, so trajectories and counters equal the graph path's bit
+// for bit.
 template <int BLOCK, int TPA>
-__global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n, int max_steps, int4 *qf0,
-                                                          int4 *qf1, int parity, double lag, GridBarrier *bar,
-                                                          int *out) {
+__global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n, int4 *qf0, int4 *qf1, double lag,
+                                                          GridBarrier *bar, int *out) {
   __shared__ int go;
   __shared__ volatile int found;
   const Thermo th{};
@@ -2022,13 +1994,16 @@ __global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n
   const long long stride = (long long)gridDim.x * BLOCK;
   const int gtid = blockIdx.x * BLOCK + threadIdx.x, gthreads = gridDim.x * BLOCK;
   Status *st = a.st;
-  volatile int *decision = &out[2];
+  volatile int *decision = &out[0];
+  int parity = *(volatile int *)&st->fix_parity;
   int steps = 0;
-  for (; steps < max_steps; steps++) {
+  for (;; steps++) {
     // 0: leave this step to the caller; 1: take it; 2: check displacements first
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       int g = 0;
-      if (take_step_alone(st, b)) {
+      if (st->steps >= st->target_steps) {
+        g = 0;
+      } else if (take_step_alone(st, b)) {
         g = 1;
       } else if (!st->error && !st->list_stale) {
         int disp = 0;
@@ -2111,9 +2086,37 @@ __global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n
     if (!grid_barrier(bar, st, kBarrierPolls)) break;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    out[0] = steps;
-    out[1] = parity;
+    st->fix_parity = parity;
+    st->persistent_steps += steps;
   }
+}
+
+// The rebuild step of the persistent pipeline: queued after each persistent
+// launch, it runs only when that launch stopped for a rebuild (a stale
+// list, no error, steps left).  Then it takes expiry_decide's stale-list
+// branch (want_build, the |v| maximum cleared) and the graph body rebuilds,
+// packs buffer 0 and runs the fused step from it.
+static __global__ void k_rebuild_guard(Arrays a, Box b, cudaGraphConditionalHandle h_run) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Status *st = a.st;
+  int run = !st->error && st->list_stale && st->steps < st->target_steps;
+  if (run) {
+    int disp = 0;
+    run = expiry_decide(st, b, &disp) && !st->error;
+  }
+  cudaGraphSetConditional(h_run, run);
+}
+
+static __global__ void k_set_parity(Arrays a, int parity) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && !a.st->error) a.st->fix_parity = parity;
+}
+
+// Start of a persistent pipeline run: the step count to stop at and the
+// buffer the next fused step reads.
+static __global__ void k_set_target(Arrays a, long long target, int parity) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  a.st->target_steps = target;
+  a.st->fix_parity = parity;
 }
 
 // Kinetic energy partials (KineticEnergyObserver, src/observer.cc:4-15).
