@@ -79,7 +79,7 @@ typedef struct {
                                and problem shape, at the first step */
   int build_block;          /* list build: threads per block, 64, 128 or 256; 0
                                (default) = chosen by timing, as threads_per_atom */
-  int build_threads_per_atom; /* list build: lanes per atom, 1, 2 or 4 (the rows are the
+  int build_threads_per_atom; /* list build: lanes per atom, 1, 2, 4 or 8 (the rows are the
                                same for every choice); 0 (default) = chosen by timing
                                together with build_block */
   int step_mode;            /* how mdg_calculate runs FP32-mixed NVE steps:

@@ -25,6 +25,10 @@ namespace {
 
 constexpr int kBlock = 256;       // streaming kernels
 constexpr int kForceBlock = 128;  // pair kernels
+#ifndef MDG_PERSIST_BLOCK
+#define MDG_PERSIST_BLOCK 128
+#endif
+constexpr int kPersistBlock = MDG_PERSIST_BLOCK;  // the persistent pass (fewer, larger blocks: cheaper grid barriers)
 constexpr int kScanBlock = 1024;  // cells per tile of the cell-count scan
 constexpr int kStepsPerGraph = 20;
 // Staged atoms per force block for stage_atoms = -1: 36 KB, six blocks per SM.
@@ -259,7 +263,8 @@ template <int BLOCK>
 void launch_list_build_block(mdg_handle *h, cudaStream_t s, int lanes) {
   const int n = h->n;
   const int nb = (int)std::max<long long>(1, ((long long)n * lanes + BLOCK - 1) / BLOCK);
-  if (lanes == 4) k_build<BLOCK, false, false, 4><<<nb, BLOCK, 0, s>>>(h->a, h->box, n);
+  if (lanes == 8) k_build<BLOCK, false, false, 8><<<nb, BLOCK, 0, s>>>(h->a, h->box, n);
+  else if (lanes == 4) k_build<BLOCK, false, false, 4><<<nb, BLOCK, 0, s>>>(h->a, h->box, n);
   else if (lanes == 2) k_build<BLOCK, false, false, 2><<<nb, BLOCK, 0, s>>>(h->a, h->box, n);
   else k_build<BLOCK, false, false, 1><<<nb, BLOCK, 0, s>>>(h->a, h->box, n);
 }
@@ -714,7 +719,7 @@ mdg_status autotune(mdg_handle *h) {
   if (bb == 0 || bl == 0) {
     float best = -1.f;
     int bb_best = 0, bl_best = 0;
-    const int blocks[3] = {64, 128, 256}, lanes[3] = {1, 2, 4};
+    const int blocks[3] = {64, 128, 256}, lanes[4] = {1, 2, 4, 8};
     for (int cb : blocks) {
       if (bb != 0 && cb != bb) continue;
       for (int cl : lanes) {
@@ -757,11 +762,11 @@ mdg_status autotune(mdg_handle *h) {
 template <int TPA>
 int persistent_grid_of(mdg_handle *h) {
   int per_sm = 0, sms = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nve_persistent<kForceBlock, TPA>, kForceBlock, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nve_persistent<kPersistBlock, TPA>, kPersistBlock, 0) !=
           cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->prm.device) != cudaSuccess)
     return 0;
-  const long long need = ((long long)h->n * TPA + kForceBlock - 1) / kForceBlock;
+  const long long need = ((long long)h->n * TPA + kPersistBlock - 1) / kPersistBlock;
   return (int)std::min<long long>(need, (long long)per_sm * sms);
 }
 
@@ -781,7 +786,7 @@ bool use_persistent(mdg_handle *h) {
   const int g = persistent_grid(h);
   if (g <= 0) return false;
   if (h->prm.step_mode == MDG_STEPS_PERSISTENT) return true;
-  return (long long)g * kForceBlock >= (long long)h->n * tpa;
+  return (long long)g * kPersistBlock >= (long long)h->n * tpa;
 }
 
 // One persistent launch, queued (no wait): it takes steps until one needs a
@@ -794,9 +799,9 @@ mdg_status enqueue_persistent_tpa(mdg_handle *h) {
   int n = h->n;
   int4 *q0 = h->a.qfix, *q1 = h->a.qfix2;
   double lag = step_lag(h);  // the ghost copies' age at a step's displacement check
-  void *args[] = {&h->a, &h->box, &n, &q0, &q1, &lag, &h->d_bar, &h->d_pout};
-  CUDA_TRY(h, cudaLaunchCooperativeKernel((const void *)k_nve_persistent<kForceBlock, TPA>, dim3(grid),
-                                          dim3(kForceBlock), args, 0, h->stream));
+  void *args[] = {&h->a, &h->box, &n, &q0, &q1, &lag, &h->d_bar};
+  CUDA_TRY(h, cudaLaunchCooperativeKernel((const void *)k_nve_persistent<kPersistBlock, TPA>, dim3(grid),
+                                          dim3(kPersistBlock), args, 0, h->stream));
   h->kernel_launches++;
   return MDG_OK;
 }
@@ -861,8 +866,11 @@ mdg_status run_persistent(mdg_handle *h, long long target, Status *st) {
       CUDA_TRY(h, cudaGraphLaunch(h->rebuild_exec, h->stream));
       h->kernel_launches += 2;
     }
+    const long long rebuilds = st->rebuilds;
     if ((r = read_status(h, st))) return r;
-    if (st->steps > steps) h->steps_per_cycle = std::max(1.0, (double)(st->steps - steps) / pairs);
+    // each launch pair ends with a rebuild, except the last: pairs that did
+    // work = rebuilds + 1
+    if (st->steps > steps) h->steps_per_cycle = std::max(1.0, (double)(st->steps - steps) / (st->rebuilds - rebuilds + 1));
     if (st->error || st->steps == steps) break;
     steps = st->steps;
   }
@@ -912,7 +920,7 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
        prm->threads_per_atom != 4) ||
       (prm->build_block != 0 && prm->build_block != 64 && prm->build_block != 128 && prm->build_block != 256) ||
       (prm->build_threads_per_atom != 0 && prm->build_threads_per_atom != 1 && prm->build_threads_per_atom != 2 &&
-       prm->build_threads_per_atom != 4) ||
+       prm->build_threads_per_atom != 4 && prm->build_threads_per_atom != 8) ||
       prm->step_mode < MDG_STEPS_AUTO || prm->step_mode > MDG_STEPS_PERSISTENT)
     return MDG_ERR_INVALID_ARGUMENT;
   for (int d = 0; d < 3; d++)

@@ -106,6 +106,7 @@ struct Status {
   long long target_steps;
   int fix_parity;
   long long persistent_steps;
+  unsigned long long vmax2_ring[3];  // the persistent pass's |v| maxima, step k in slot k % 3
 };
 
 // An executor the reference's projects run after every Calculate() (on the
@@ -1918,35 +1919,45 @@ struct GridBarrier {
   unsigned gen;
 };
 
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Every block of the (cooperative, fully resident) grid arrives; false if
+// this block gave up waiting after `limit` polls (kErrTimeout is set).  The
+// block's writes before the barrier are visible to every block after it:
+// a gpu-scope fence before the arrival, acquire loads while waiting.
 __device__ __forceinline__ bool grid_barrier(GridBarrier *g, Status *st, long long limit) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
-    const unsigned gen = *(volatile unsigned *)&g->gen;
+    const unsigned gen = ld_acquire_gpu(&g->gen);
     __threadfence();
     if (atomicAdd(&g->count, 1u) + 1u == gridDim.x) {
-      g->count = 0u;
+      g->count = 0u;  // no block arrives at the next barrier before gen moves
       __threadfence();
       atomicAdd(&g->gen, 1u);
     } else {
       long long polls = 0;
-      while (*(volatile unsigned *)&g->gen == gen) {
+      while (ld_acquire_gpu(&g->gen) == gen) {
         if (++polls > limit) {
           atomicOr(&st->error, kErrTimeout);
           ok = 0;
           break;
         }
-        __nanosleep(64);
+        __nanosleep(20);
       }
     }
-    __threadfence();
   }
   __syncthreads();
   return ok != 0;
 }
 
-// About a second of polling at 64 ns per poll: a step takes microseconds.
+// About a second of polling (a poll and a 20 ns sleep take some 60 ns): a
+// step takes microseconds.
 constexpr long long kBarrierPolls = 16000000ll;
 
 // The expiry test of PairList::IsPairListExpired (k_expiry's arithmetic)
@@ -1967,26 +1978,38 @@ __device__ __forceinline__ bool take_step_alone(Status *st, const Box &b) {
   return true;
 }
 
-// FP32-mixed NVE steps in one cooperative launch, for
-// systems small enough that per-step launch latency dominates: each step is
-// the fused pass of k_force_fp32<.., kKick, 2, TPA> over all atoms
-// (grid-stride), between grid barriers.  Block 0 takes the expiry decision
-// (take_step_alone, else expiry_decide); a step whose skin budget is spent
-// runs the displacement check of PairList::CheckByDisplacement in the same
-// launch, as k_disp_max, k_disp_collect and k_disp_pairs do it (copies
-// dated `lag` back), each phase ending in a grid barrier.  The pass stops
-// before the first step that needs a rebuild -- it marks the list stale, so
-// the caller's ordinary step rebuilds without deciding again -- and before
-// any error, or when the step count reaches Status::target_steps.  The
+// FP32-mixed NVE steps in one cooperative launch, for systems small enough
+// that per-step launch latency dominates: each step is the fused pass of
+// k_force_fp32<.., kKick, 2, TPA> over all atoms (grid-stride) followed by
+// one grid barrier.  Every decision of PairList::IsPairListExpired and
+// CheckByDisplacement is a function of values every block holds or reads
+// after a barrier, so every block takes it by itself:
+// - the skin budget lives in a register (budget -= 2 vmax dt while
+//   positive; a check once it is negative);
+// - the step's |v| maximum comes from a ring of three slots (pass k fills
+//   slot k % 3; block 0 clears slot k + 1 during step k, which no block
+//   reads any more and none fills before the next barrier);
+// - a displacement check runs as k_disp_max, k_disp_collect and
+//   k_disp_pairs do it (copies dated `lag` back), three phases each ending
+//   in a grid barrier, and every block reads the verdict (want_build) after
+//   the last one; block 0 clears the check's counters after it (the next
+//   check starts at least one barrier later) and want_build while the next
+//   check's first phase runs.
+// The pass stops before the first step that needs a rebuild -- it marks the
+// list stale, so the caller's ordinary step rebuilds without deciding again
+// -- before a step whose atom is too fast (the caller's step reports it),
+// or when the step count reaches Status::target_steps; block 0 then writes
+// the budget, the |v| maximum, the counters and the buffer parity back.
+// Errors raised inside the passes stop the work of later passes (they
+// check the flag) and are reported by the caller; the decisions never read
+// the flag, which a block may raise while another still decides.  The
 // fixed-point buffer the next step reads comes from, and goes back to,
-// Status::fix_parity (0: qf0, 1: qf1); out[0] broadcasts block 0's
-// decisions.  The arithmetic is k_force_fp32's and the decisions are the
-// graph path's, so trajectories and counters equal the graph path's bit
-// for bit.
+// Status::fix_parity (0: qf0, 1: qf1).  The arithmetic is k_force_fp32's
+// and the decisions are the graph path's, so trajectories and counters
+// equal the graph path's bit for bit.
 template <int BLOCK, int TPA>
 __global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n, int4 *qf0, int4 *qf1, double lag,
-                                                          GridBarrier *bar, int *out) {
-  __shared__ int go;
+                                                          GridBarrier *bar) {
   __shared__ volatile int found;
   const Thermo th{};
   const PairConst k = pair_const(b.fix_scale, b.rc2f, b.c2x8f);
@@ -1994,29 +2017,44 @@ __global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n
   const long long stride = (long long)gridDim.x * BLOCK;
   const int gtid = blockIdx.x * BLOCK + threadIdx.x, gthreads = gridDim.x * BLOCK;
   Status *st = a.st;
-  volatile int *decision = &out[0];
+  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  // the values the decisions start from, read by every block before any is
+  // written (the first barrier)
   int parity = *(volatile int *)&st->fix_parity;
-  int steps = 0;
-  for (;; steps++) {
-    // 0: leave this step to the caller; 1: take it; 2: check displacements first
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      int g = 0;
-      if (st->steps >= st->target_steps) {
-        g = 0;
-      } else if (take_step_alone(st, b)) {
-        g = 1;
-      } else if (!st->error && !st->list_stale) {
-        int disp = 0;
-        expiry_decide(st, b, &disp);  // spends the budget; a too-fast atom is an error
-        g = st->error ? 0 : (disp ? 2 : 1);
+  double budget = *(volatile double *)&st->budget;
+  unsigned long long vmax2 = *(volatile unsigned long long *)&st->vmax2_bits;
+  const long long steps0 = *(volatile long long *)&st->steps;
+  const long long target = *(volatile long long *)&st->target_steps;
+  const bool startable = !*(volatile int *)&st->error && !*(volatile int *)&st->list_stale;
+  double sim_time = st->sim_time;  // block 0's copy
+  if (lead) {
+    st->vmax2_ring[0] = st->vmax2_ring[1] = 0ull;
+    st->dr2max_bits = 0ull;
+    st->cand_weighted = 0;
+    st->cand_n = 0;
+  }
+  if (!grid_barrier(bar, st, kBarrierPolls)) return;
+  bool stale = false, checked = false;
+  long long taken = 0, checks = 0;
+  for (;; taken++) {
+    // 0: stop; 1: take the step; 2: check displacements first
+    int g = 0;
+    if (startable && steps0 + taken < target) {
+      if (budget > 0.0) {
+        const double cost = skin_cost(sqrt(__longlong_as_double((long long)vmax2)), b.dt);
+        if (cost <= b.buffer_length) {  // else too fast: the caller's step reports it
+          budget = dsub(budget, cost);
+          g = budget < 0.0 ? 2 : 1;
+        }
+      } else {
+        g = budget < 0.0 ? 2 : 1;
       }
-      *decision = g;
-      __threadfence();
     }
-    if (!grid_barrier(bar, st, kBarrierPolls)) break;
-    if (threadIdx.x == 0) go = *decision;
-    __syncthreads();
-    if (go == 2) {
+    checked = false;
+    if (g == 2) {
+      checks++;
+      checked = true;
+      if (lead) st->want_build = 0;
       double d2 = 0.0;
       for (int i = gtid; i < n; i += gthreads)
         for_each_copy(copy_view(a), b.L, i, lag, [&](int, double x) { d2 = fmax(d2, x); });
@@ -2037,8 +2075,7 @@ __global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n
       __syncthreads();
       const long long tn = st->total_images;
       const int nl = (int)((tn > b.check_list_length) ? b.check_list_length : tn);
-      const int weighted = *(volatile int *)&st->cand_weighted;
-      if (weighted >= nl) {
+      if (*(volatile int *)&st->cand_weighted >= nl) {
         if (threadIdx.x == 0) found = 1;
       } else {
         const int l = min(*(volatile int *)&st->cand_n, b.check_list_length);
@@ -2048,25 +2085,26 @@ __global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n
       __syncthreads();
       if (threadIdx.x == 0 && found) st->want_build = 1;
       if (!grid_barrier(bar, st, kBarrierPolls)) break;
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
-        // k_decide: a rebuild is left to the caller's ordinary step
-        const int build = !st->error && st->want_build;
-        st->vlag_set = 0;
-        if (build) st->list_stale = 1;
-        *decision = (build || st->error) ? 0 : 1;
-        __threadfence();
+      stale = *(volatile int *)&st->want_build != 0;
+      if (lead) {
+        // the check is over: its counters are free for the next one
+        st->dr2max_bits = 0ull;
+        st->cand_weighted = 0;
+        st->cand_n = 0;
+        st->vlag_set = 0;  // k_decide: the check has read the ghost copies
       }
-      if (!grid_barrier(bar, st, kBarrierPolls)) break;
-      if (threadIdx.x == 0) go = *decision;
-      __syncthreads();
+      if (stale) break;  // a rebuild is left to the caller's ordinary step
     }
-    if (!go) break;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      st->steps++;
-      st->sim_time += b.dt;
+    if (g == 0) break;
+    // the step: block 0 clears the ring slot step taken + 1 will fill
+    if (lead) {
+      st->vmax2_ring[(taken + 1) % 3] = 0ull;
+      if (!checked) st->vlag_set = 0;  // expiry_decide's clear: no check reads the copies this step
+      sim_time += b.dt;
     }
     const int4 *qf = parity ? qf1 : qf0;
     int4 *qf_next = parity ? qf0 : qf1;
+    unsigned long long *ring = &st->vmax2_ring[taken % 3];
     // warps walk whole warps of threads, so the lane shuffles stay converged
     for (long long base = (long long)blockIdx.x * BLOCK + (threadIdx.x & ~31); base < nthreads; base += stride) {
       const long long t = base + (threadIdx.x & 31);
@@ -2080,14 +2118,29 @@ __global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n
         fp32_row<TPA>(f, (a.nnbr[i] + 3) >> 2, sub, pi, k, Fx, Fy, Fz);
         if (sub == 0) fp32_finish<kKick, 2>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
       }
-      warp_max_to(&st->vmax2_bits, v2);
+      warp_max_to(ring, v2);
     }
     parity ^= 1;
-    if (!grid_barrier(bar, st, kBarrierPolls)) break;
+    if (!grid_barrier(bar, st, kBarrierPolls)) {
+      taken++;
+      break;
+    }
+    vmax2 = *(volatile unsigned long long *)ring;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (lead) {
+    st->steps = steps0 + taken;
+    st->sim_time = sim_time;
+    st->budget = budget;
+    // expiry_decide's clear at a step that stopped for a rebuild; else the
+    // last pass's maximum, which the next decision reads
+    st->vmax2_bits = checked && stale ? 0ull : vmax2;
+    st->disp_checks += checks;
+    if (stale) {
+      st->list_stale = 1;
+      st->want_build = 1;
+    }
     st->fix_parity = parity;
-    st->persistent_steps += steps;
+    st->persistent_steps += taken;
   }
 }
 

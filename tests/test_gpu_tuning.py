@@ -24,7 +24,7 @@ def _system(st, **kw):
 @pytest.mark.parametrize("rho", [0.5, 0.8442])
 def test_lanes_and_blocks_bit_identical(rho):
     st = W.fcc_liquid(8, rho, 1.0, seed=71, jitter=0.06, rc=2.5, dt=0.005)
-    shapes = [(1, 64, 2), (2, 128, 4), (4, 256, 1), (1, 128, 4)]
+    shapes = [(1, 64, 2), (2, 128, 4), (4, 256, 1), (1, 128, 4), (2, 64, 8)]
     forces, states, pairs = [], [], []
     for tpa, bb, bl in shapes:
         s = _system(st, threads_per_atom=tpa, build_block=bb, build_threads_per_atom=bl)
@@ -69,7 +69,7 @@ def test_autotune_picks_a_shape_and_keeps_the_trajectory():
     info = a.info()
     assert info["threads_per_atom"] in (1, 2, 4)
     assert info["build_block"] in (64, 128, 256)
-    assert info["build_threads_per_atom"] in (1, 2, 4)
+    assert info["build_threads_per_atom"] in (1, 2, 4, 8)
     qa, va = a.state_by_id()
     qb, vb = b.state_by_id()
     assert np.array_equal(qa, qb) and np.array_equal(va, vb)
@@ -96,7 +96,7 @@ def test_ensemble_lanes_bit_identical():
 
 
 @pytest.mark.parametrize("field,value", [("threads_per_atom", 3), ("build_block", 100),
-                                         ("build_threads_per_atom", 8)])
+                                         ("build_threads_per_atom", 16)])
 def test_invalid_shapes_rejected(field, value):
     st = W.fcc_liquid(5, 0.5, 1.0, seed=75, rc=2.5)
     with pytest.raises(M.MdgError) as e:
@@ -106,9 +106,10 @@ def test_invalid_shapes_rejected(field, value):
 
 @pytest.mark.parametrize("tpa", [1, 4])
 def test_persistent_steps_equal_graph_steps(tpa):
-    # the cooperative multi-step pass runs the fused NVE step back to back
-    # and hands the steps that need the displacement check or a rebuild to
-    # the ordinary path: the trajectory is the graph path's bit for bit
+    # the cooperative multi-step pass runs the fused NVE step back to back,
+    # takes the displacement checks itself and hands the steps that need a
+    # rebuild to the queued rebuild step: the trajectory, the rebuild steps
+    # and the check count are the graph path's
     st = W.fcc_liquid(12, 0.5, 1.0, seed=76, jitter=0.05, rc=2.5, dt=0.005)
     a = _system(st, threads_per_atom=tpa, step_mode=M.STEPS_GRAPHS)
     b = _system(st, threads_per_atom=tpa, step_mode=M.STEPS_PERSISTENT)
@@ -120,5 +121,6 @@ def test_persistent_steps_equal_graph_steps(tpa):
     assert np.array_equal(qa, qb) and np.array_equal(va, vb)
     ia, ib = a.info(), b.info()
     assert ia["rebuilds"] == ib["rebuilds"] and ia["displacement_checks"] == ib["displacement_checks"]
+    assert ia["simulation_time"] == ib["simulation_time"] and ia["buffer_left"] == ib["buffer_left"]
     assert ib["persistent_steps"] > 100 and ia["persistent_steps"] == 0
     assert ib["steps"] == 200
