@@ -86,9 +86,11 @@ typedef struct {
                                MDG_STEPS_AUTO (default): persistent when every atom's lanes
                                fit in one wave of co-resident blocks, else graphs;
                                MDG_STEPS_GRAPHS: CUDA graphs with conditional rebuild nodes;
-                               MDG_STEPS_PERSISTENT: one cooperative launch runs the steps
-                               back to back until one needs the displacement check or a
-                               rebuild, which then runs as an ordinary step.  Same results. */
+                               MDG_STEPS_PERSISTENT: cooperative launches run the steps
+                               back to back, displacement checks included (one lane per
+                               atom from 16,384 atoms, 2 or 4 below); each stops at a step
+                               that needs a rebuild, which a queued graph takes, and the
+                               next launch follows without a host wait.  Same results. */
 } mdg_params;
 
 enum { MDG_STEPS_AUTO = 0, MDG_STEPS_GRAPHS = 1, MDG_STEPS_PERSISTENT = 2 };

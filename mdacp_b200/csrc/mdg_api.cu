@@ -25,6 +25,7 @@ namespace {
 
 constexpr int kBlock = 256;       // streaming kernels
 constexpr int kForceBlock = 128;  // pair kernels
+constexpr int kScanSingleCells = 16384;  // cell grids up to this size are scanned by one block
 #ifndef MDG_PERSIST_BLOCK
 #define MDG_PERSIST_BLOCK 128
 #endif
@@ -255,7 +256,7 @@ double step_lag(const mdg_handle *h) {
 // pack: where to put the coming step's first-drift positions after the
 // rebuild (the fused FP32 NVE step), or nullptr.
 // Kernels of one rebuild (launch_build).
-int build_kernels(const mdg_handle *h) { return h->a.stage_cap > 0 ? 11 : 10; }
+int build_kernels(const mdg_handle *h) { return (h->ncell <= kScanSingleCells ? 9 : 11) + (h->a.stage_cap > 0 ? 1 : 0); }
 
 // The list build alone (the rows of the atoms' current cell order), with
 // `block` threads per block and `lanes` threads per atom.
@@ -278,20 +279,20 @@ void launch_list_build(mdg_handle *h, cudaStream_t s, int block, int lanes) {
 void launch_build(mdg_handle *h, cudaStream_t s, int4 *pack = nullptr) {
   const int n = h->n;
   Arrays &a = h->a;
-  k_build_begin<<<1, 32, 0, s>>>(a);
-  cudaMemsetAsync(a.cell_count, 0, sizeof(int) * h->ncell, s);
+  k_build_begin_clear<kBlock><<<std::min(blocks_for(h->ncell, kBlock), 1024), kBlock, 0, s>>>(a, h->ncell);
   k_cell_assign<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, h->box, n);
-  const int ntiles = blocks_for(h->ncell, kScanBlock);
-  k_scan_tiles<kScanBlock><<<ntiles, kScanBlock, 0, s>>>(a, h->ncell, h->d_tiles);
-  k_scan_tile_sums<kScanBlock><<<1, kScanBlock, 0, s>>>(a, h->ncell, h->d_tiles, ntiles);
-  k_scan_add<kScanBlock><<<ntiles, kScanBlock, 0, s>>>(a, h->ncell, h->d_tiles);
+  if (h->ncell <= kScanSingleCells) {
+    k_scan_single<kScanBlock><<<1, kScanBlock, 0, s>>>(a, h->ncell);
+  } else {
+    const int ntiles = blocks_for(h->ncell, kScanBlock);
+    k_scan_tiles<kScanBlock><<<ntiles, kScanBlock, 0, s>>>(a, h->ncell, h->d_tiles);
+    k_scan_tile_sums<kScanBlock><<<1, kScanBlock, 0, s>>>(a, h->ncell, h->d_tiles, ntiles);
+    k_scan_add<kScanBlock><<<ntiles, kScanBlock, 0, s>>>(a, h->ncell, h->d_tiles);
+  }
   k_scatter<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, n);
   k_sort_cells<<<blocks_for(h->ncell * 32, kBlock), kBlock, 0, s>>>(a, h->box, h->ncell);
   k_permute<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, h->box, n, pack);
-  cudaMemcpyAsync(a.q, a.q_tmp, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
-  cudaMemcpyAsync(a.v, a.v_tmp, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
-  cudaMemcpyAsync(a.ids, a.ids_tmp, sizeof(int) * n, cudaMemcpyDeviceToDevice, s);
-  cudaMemcpyAsync(a.type, a.type_tmp, sizeof(int) * n, cudaMemcpyDeviceToDevice, s);
+  k_copy_back<kBlock><<<blocks_for(n, kBlock), kBlock, 0, s>>>(a, n);
   if (a.stage_cap > 0) {
     static_assert(kForceBlock == kStageBlock, "the build writes stage rows per force block");
     k_stage_plan<kBlock><<<blocks_for(blocks_for(n, kStageBlock), kBlock), kBlock, 0, s>>>(a, h->box, n);
@@ -770,9 +771,16 @@ int persistent_grid_of(mdg_handle *h) {
   return (int)std::min<long long>(need, (long long)per_sm * sms);
 }
 
+// Lanes per atom of the persistent pass.  Its steps end in a grid barrier
+// whose cost grows with the block count, so it takes fewer lanes than the
+// graph path's tuned force pass: one per atom from 16,384 atoms (measured
+// on the 32,000-atom liquid: 31 us per step with one lane, 35-40 with two),
+// more for smaller systems.  Every lane count gives the same forces.
+int persistent_tpa(const mdg_handle *h) { return h->n >= 16384 ? 1 : (h->n >= 8192 ? 2 : 4); }
+
 int persistent_grid(mdg_handle *h) {
   if (h->persist_grid < 0) {
-    const int tpa = h->tpa > 0 ? h->tpa : 1;
+    const int tpa = persistent_tpa(h);
     h->persist_grid = tpa == 4 ? persistent_grid_of<4>(h) : (tpa == 2 ? persistent_grid_of<2>(h) : persistent_grid_of<1>(h));
   }
   return h->persist_grid;
@@ -782,7 +790,7 @@ int persistent_grid(mdg_handle *h) {
 // one wave of resident blocks covers every atom's lanes.
 bool use_persistent(mdg_handle *h) {
   if (!fused_step(h) || h->prm.step_mode == MDG_STEPS_GRAPHS) return false;
-  const int tpa = h->tpa > 0 ? h->tpa : 1;
+  const int tpa = persistent_tpa(h);
   const int g = persistent_grid(h);
   if (g <= 0) return false;
   if (h->prm.step_mode == MDG_STEPS_PERSISTENT) return true;
@@ -807,7 +815,7 @@ mdg_status enqueue_persistent_tpa(mdg_handle *h) {
 }
 
 mdg_status enqueue_persistent(mdg_handle *h) {
-  const int tpa = h->tpa > 0 ? h->tpa : 1;
+  const int tpa = persistent_tpa(h);
   return tpa == 4 ? enqueue_persistent_tpa<4>(h) : (tpa == 2 ? enqueue_persistent_tpa<2>(h) : enqueue_persistent_tpa<1>(h));
 }
 

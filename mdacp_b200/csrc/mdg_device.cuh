@@ -827,6 +827,24 @@ __global__ void __launch_bounds__(BLOCK) k_scan_add(Arrays a, int ncell, const i
   if (c < ncell && blockIdx.x > 0) a.cell_start[c] += tile_sum[blockIdx.x];
 }
 
+// The same in one block, for grids of few cells: the carry runs over
+// chunks of BLOCK cells (one launch instead of three).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scan_single(Arrays a, int ncell) {
+  __shared__ int total;
+  if (a.st->error) return;
+  int carry = 0;
+  for (int base = 0; base < ncell; base += BLOCK) {
+    const int c = base + threadIdx.x;
+    const int x = c < ncell ? a.cell_count[c] : 0;
+    const int ex = block_exclusive_scan<BLOCK>(x, &total);
+    if (c < ncell) a.cell_start[c] = carry + ex;
+    carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) a.cell_start[ncell] = carry;
+}
+
 // Rebuild 3/6: scatter old slots to their cell ranges.
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_scatter(Arrays a, int n) {
@@ -968,22 +986,51 @@ __device__ __forceinline__ void build_range(const float4 *__restrict__ qloc, con
     return keep;
   };
   if (BTPA == 1) {
-    auto test = [&](int j, const float4 &l) {
-      if (keep_of(j, l)) {
-        emit(j, cnt);
-        cnt++;
-      }
+    // four candidates at a time: the four prefilter tests are independent
+    // (one pass over them), the rare band candidates are decided in one
+    // branch, then the kept ones are filed in slot order
+    auto prefilter = [&](int j, const float4 &l, float &r2) {
+      const float ex = l.x + bx, ey = l.y + by, ez = l.z + bz;
+      r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+      bool keep = r2 <= b.sl2_hi;
+      if (SELF) keep = keep && j != i;
+      return keep;
     };
     int j = beg;
     for (; j + 4 <= end; j += 4) {
       const float4 l0 = __ldg(qloc + j), l1 = __ldg(qloc + j + 1), l2 = __ldg(qloc + j + 2),
                    l3 = __ldg(qloc + j + 3);
-      test(j, l0);
-      test(j + 1, l1);
-      test(j + 2, l2);
-      test(j + 3, l3);
+      float r0, r1, r2, r3;
+      bool k0 = prefilter(j, l0, r0), k1 = prefilter(j + 1, l1, r1), k2 = prefilter(j + 2, l2, r2),
+           k3 = prefilter(j + 3, l3, r3);
+      if (NEED) {
+        k0 = k0 && (mult[j] & need) == need;
+        k1 = k1 && (mult[j + 1] & need) == need;
+        k2 = k2 && (mult[j + 2] & need) == need;
+        k3 = k3 && (mult[j + 3] & need) == need;
+      }
+      const float lo = b.sl2_lo;
+      if ((k0 && r0 >= lo) || (k1 && r1 >= lo) || (k2 && r2 >= lo) || (k3 && r3 >= lo)) {
+        if (k0 && r0 >= lo) k0 = band_test(q, i, j, shift, b);
+        if (k1 && r1 >= lo) k1 = band_test(q, i, j + 1, shift, b);
+        if (k2 && r2 >= lo) k2 = band_test(q, i, j + 2, shift, b);
+        if (k3 && r3 >= lo) k3 = band_test(q, i, j + 3, shift, b);
+      }
+      if (k0) emit(j, cnt);
+      cnt += k0;
+      if (k1) emit(j + 1, cnt);
+      cnt += k1;
+      if (k2) emit(j + 2, cnt);
+      cnt += k2;
+      if (k3) emit(j + 3, cnt);
+      cnt += k3;
     }
-    for (; j < end; j++) test(j, __ldg(qloc + j));
+    for (; j < end; j++) {
+      if (keep_of(j, __ldg(qloc + j))) {
+        emit(j, cnt);
+        cnt++;
+      }
+    }
   } else {
     const int lane = threadIdx.x & 31, sub = lane & (BTPA - 1), first = lane & ~(BTPA - 1);
     const unsigned gmask = (BTPA == 32) ? 0xffffffffu : (((1u << BTPA) - 1u) << first);
@@ -1192,6 +1239,28 @@ static __global__ void k_build_begin(Arrays a) {
   a.st->max_row = 0;
   a.st->list_entries = 0;
   a.st->total_images = 0;
+}
+
+// k_build_begin and the clear of the cell counts in one launch.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_build_begin_clear(Arrays a, int ncell) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    a.st->max_row = 0;
+    a.st->list_entries = 0;
+    a.st->total_images = 0;
+  }
+  for (int c = blockIdx.x * BLOCK + threadIdx.x; c < ncell; c += gridDim.x * BLOCK) a.cell_count[c] = 0;
+}
+
+// The permuted state back into place (q, v, ids, types), one launch.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_copy_back(Arrays a, int n) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= n) return;
+  a.q[i] = a.q_tmp[i];
+  a.v[i] = a.v_tmp[i];
+  a.ids[i] = a.ids_tmp[i];
+  a.type[i] = a.type_tmp[i];
 }
 
 // After a build: fresh skin budget (PairList::Init, src/pairlist.cc:10-23),
