@@ -1515,15 +1515,18 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp64(Arrays a, Box b, int n, Th
     const double dt = (MODE == kForceOut) ? 1.0 : b.dt;
     double fx = 0.0, fy = 0.0, fz = 0.0;
     const int *row = a.nbr + i;
-    int j = nn > 0 ? row[0] : 0;
+    // software pipeline: the next partner's position and the entry after it
+    // are in flight while a pair term is formed
+    int jn = nn > 1 ? row[a.stride] : i;
+    double4 qn = a.q[nn > 0 ? row[0] : i];
     for (int k = 0; k < nn; k++) {
-      const int jn = (k + 1 < nn) ? row[(size_t)(k + 1) * a.stride] : 0;
-      const double4 qj = a.q[j];
+      const double4 qj = qn;
+      qn = a.q[jn];
+      jn = (k + 2 < nn) ? row[(size_t)(k + 2) * a.stride] : i;
       const double dx = dsub(image_of(qj.x, qi.x, b.L[0], b.hL[0]), qi.x);
       const double dy = dsub(image_of(qj.y, qi.y, b.L[1], b.hL[1]), qi.y);
       const double dz = dsub(image_of(qj.z, qi.z, b.L[2], b.hL[2]), qi.z);
       const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-      j = jn;
       if (r2 > b.rc2) continue;
       const double r6 = dmul(dmul(r2, r2), r2);
       const double df = dmul(dadd(ddiv(dsub(dmul(24.0, r6), 48.0), dmul(dmul(r6, r6), r2)), c2x8), dt);
