@@ -1620,18 +1620,21 @@ __device__ __forceinline__ void fp32_finish(Arrays &a, const Box &b, const Therm
 // order, so every lane holds S at the end.  Chunks past the row's end add
 // +0.0, which leaves S unchanged (S starts at +0.0 and is never -0.0).
 
-// Partner positions of a lane's groups from the global fixed-point copy,
-// software-pipelined: while a group is summed, the next group's positions
-// and the list entries of the group after it are in flight (the gathers
-// are the pass's long-latency loads, the list its one stream from HBM).
-// Group -1 is none: its entries are the atom itself.
+// Partner positions of a lane's groups from the global fixed-point copy.
+// The list entries of the group after the next are in flight while a group
+// is summed (the list is the pass's one stream from HBM); with AHEAD the
+// next group's positions are too (software pipeline: the gathers are the
+// pass's long-latency loads; four more int4 registers).  Group -1 is none:
+// its entries are the atom itself.
+template <bool AHEAD = true>
 struct GlobalGroups {
   const int *row;  // nbr + atom
   int st;          // list stride
   const int4 *qf;
   int self;
+  int n0, n1, n2, n3;      // entries of the current group (without AHEAD)
   int m0, m1, m2, m3;      // entries of the next group
-  int4 c0, c1, c2, c3;     // positions of the current group
+  int4 c0, c1, c2, c3;     // positions of the current group (with AHEAD)
   __device__ __forceinline__ void load(int g, int &x0, int &x1, int &x2, int &x3) const {
     if (g < 0) {
       x0 = x1 = x2 = x3 = self;
@@ -1645,25 +1648,37 @@ struct GlobalGroups {
   }
   // the lane's first two groups
   __device__ __forceinline__ void start(int ga, int gb) {
-    int n0, n1, n2, n3;
     load(ga, n0, n1, n2, n3);
-    c0 = __ldg(qf + n0);
-    c1 = __ldg(qf + n1);
-    c2 = __ldg(qf + n2);
-    c3 = __ldg(qf + n3);
+    if (AHEAD) {
+      c0 = __ldg(qf + n0);
+      c1 = __ldg(qf + n1);
+      c2 = __ldg(qf + n2);
+      c3 = __ldg(qf + n3);
+    }
     load(gb, m0, m1, m2, m3);
   }
-  // positions of the lane's current group; the next group's positions and
-  // the entries of the group after it (gnext) start loading
+  // positions of the lane's current group; the entries of the group after
+  // the next (gnext) start loading, with AHEAD also the next group's positions
   __device__ __forceinline__ void take(int gnext, int4 &p0, int4 &p1, int4 &p2, int4 &p3) {
-    p0 = c0;
-    p1 = c1;
-    p2 = c2;
-    p3 = c3;
-    c0 = __ldg(qf + m0);
-    c1 = __ldg(qf + m1);
-    c2 = __ldg(qf + m2);
-    c3 = __ldg(qf + m3);
+    if (AHEAD) {
+      p0 = c0;
+      p1 = c1;
+      p2 = c2;
+      p3 = c3;
+      c0 = __ldg(qf + m0);
+      c1 = __ldg(qf + m1);
+      c2 = __ldg(qf + m2);
+      c3 = __ldg(qf + m3);
+    } else {
+      p0 = __ldg(qf + n0);
+      p1 = __ldg(qf + n1);
+      p2 = __ldg(qf + n2);
+      p3 = __ldg(qf + n3);
+      n0 = m0;
+      n1 = m1;
+      n2 = m2;
+      n3 = m3;
+    }
     load(gnext, m0, m1, m2, m3);
   }
 };
@@ -1841,7 +1856,7 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32(Arrays a, Box b, int n, Th
   if (i < n && !err) {
     const int4 pi = qf[i];
     double Fx, Fy, Fz;
-    GlobalGroups f{a.nbr + i, a.stride, qf, i};
+    GlobalGroups<> f{a.nbr + i, a.stride, qf, i};
     fp32_row<TPA>(f, (a.nnbr[i] + 3) >> 2, sub, pi, pair_const(b.fix_scale, b.rc2f, b.c2x8f), Fx, Fy, Fz);
     if (sub == 0) fp32_finish<MODE, DRIFT>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
   }
@@ -1969,7 +1984,7 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32_staged(Arrays a, Box b, in
       fp32_row<1>(f, G, 0, pi, k, Fx, Fy, Fz);
       if (f.bad) atomicOr(&a.st->error, kErrStage);
     } else {
-      GlobalGroups f{a.nbr + i, a.stride, qf, i};
+      GlobalGroups<> f{a.nbr + i, a.stride, qf, i};
       fp32_row<1>(f, G, 0, pi, k, Fx, Fy, Fz);
     }
     fp32_finish<MODE, DRIFT>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
@@ -2186,7 +2201,7 @@ __global__ void __launch_bounds__(BLOCK) k_nve_persistent(Arrays a, Box b, int n
       if (t < nthreads && !err) {
         const int4 pi = qf[i];
         double Fx, Fy, Fz;
-        GlobalGroups f{a.nbr + i, a.stride, qf, i};
+        GlobalGroups<> f{a.nbr + i, a.stride, qf, i};
         fp32_row<TPA>(f, (a.nnbr[i] + 3) >> 2, sub, pi, k, Fx, Fy, Fz);
         if (sub == 0) fp32_finish<kKick, 2>(a, b, th, i, Fx, Fy, Fz, qf_next, v2, ke);
       }
