@@ -971,7 +971,7 @@ __device__ __forceinline__ bool band_test(const double4 *__restrict__ q, int i, 
 // and the lanes file the ones they keep in slot order through a ballot over
 // the atom's lanes, so the row is the same for every lane count; cnt stays
 // equal on all of them.
-template <bool NEED, bool SELF, int BTPA, typename Emit>
+template <bool NEED, bool SELF, int BTPA, bool PIPE, typename Emit>
 __device__ __forceinline__ void build_range(const float4 *__restrict__ qloc, const double4 *__restrict__ q,
                                             const unsigned char *__restrict__ mult, int beg, int end, float bx,
                                             float by, float bz, int need, int shift, const Box &b, int i, int &cnt,
@@ -988,7 +988,8 @@ __device__ __forceinline__ void build_range(const float4 *__restrict__ qloc, con
   if (BTPA == 1) {
     // four candidates at a time: the four prefilter tests are independent
     // (one pass over them), the rare band candidates are decided in one
-    // branch, then the kept ones are filed in slot order
+    // branch, then the kept ones are filed in slot order; the loads run one
+    // batch ahead
     auto prefilter = [&](int j, const float4 &l, float &r2) {
       const float ex = l.x + bx, ey = l.y + by, ez = l.z + bz;
       r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
@@ -996,10 +997,35 @@ __device__ __forceinline__ void build_range(const float4 *__restrict__ qloc, con
       if (SELF) keep = keep && j != i;
       return keep;
     };
+    // PIPE: the next four candidates' loads are issued before this four's
+    // tests (four more float4 registers)
     int j = beg;
+    float4 n0, n1, n2, n3;
+    if (PIPE && j + 4 <= end) {
+      n0 = __ldg(qloc + j);
+      n1 = __ldg(qloc + j + 1);
+      n2 = __ldg(qloc + j + 2);
+      n3 = __ldg(qloc + j + 3);
+    }
     for (; j + 4 <= end; j += 4) {
-      const float4 l0 = __ldg(qloc + j), l1 = __ldg(qloc + j + 1), l2 = __ldg(qloc + j + 2),
-                   l3 = __ldg(qloc + j + 3);
+      float4 l0, l1, l2, l3;
+      if (PIPE) {
+        l0 = n0;
+        l1 = n1;
+        l2 = n2;
+        l3 = n3;
+        if (j + 8 <= end) {
+          n0 = __ldg(qloc + j + 4);
+          n1 = __ldg(qloc + j + 5);
+          n2 = __ldg(qloc + j + 6);
+          n3 = __ldg(qloc + j + 7);
+        }
+      } else {
+        l0 = __ldg(qloc + j);
+        l1 = __ldg(qloc + j + 1);
+        l2 = __ldg(qloc + j + 2);
+        l3 = __ldg(qloc + j + 3);
+      }
       float r0, r1, r2, r3;
       bool k0 = prefilter(j, l0, r0), k1 = prefilter(j + 1, l1, r1), k2 = prefilter(j + 2, l2, r2),
            k3 = prefilter(j + 3, l3, r3);
@@ -1064,7 +1090,7 @@ __device__ __forceinline__ void build_range(const float4 *__restrict__ qloc, con
 // rows in (dz, dy) order, then x order across the row's cells -- the cells
 // in dx order, as a 27-cell walk visits them.  Returns the partners found
 // (entries beyond the capacity are counted, not filed).
-template <bool SLAB = false, int BTPA = 1, typename Emit>
+template <bool SLAB = false, int BTPA = 1, bool PIPE = true, typename Emit>
 __device__ __forceinline__ int build_rows(const Box &b, const float4 *__restrict__ qloc,
                                           const double4 *__restrict__ q, const unsigned char *__restrict__ mult,
                                           const int *__restrict__ tab, int pc, int i, Emit &emit) {
@@ -1116,21 +1142,21 @@ __device__ __forceinline__ int build_rows(const Box &b, const float4 *__restrict
       const int *xr = tab + (size_t)(blk * ms1 + y) * (mx + 1);
       const int yz = (yc << 2) | (zc << 4);
       if (vlo < 0)  // through the -x face: the row's last cells, image shift -L
-        build_range<true, false, BTPA>(qloc, q, mult, xr[vlo + mx], xr[mx], bxm, by, bz,
+        build_range<true, false, BTPA, PIPE>(qloc, q, mult, xr[vlo + mx], xr[mx], bxm, by, bz,
                                        needed_strips(-b.L[0], sy, sz), 1 | yz, b, i, cnt, emit);
       {
         const int a0 = max(vlo, 0), a1 = min(vhi, mx);
         const int beg = xr[a0], end = xr[a1];
         const int need = needed_strips(0.0, sy, sz);
         if (dz == 0 && dy == 0)
-          build_range<false, true, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, 0, yz, b, i, cnt, emit);
+          build_range<false, true, BTPA, PIPE>(qloc, q, mult, beg, end, bx0, by, bz, 0, yz, b, i, cnt, emit);
         else if (need)
-          build_range<true, false, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, need, yz, b, i, cnt, emit);
+          build_range<true, false, BTPA, PIPE>(qloc, q, mult, beg, end, bx0, by, bz, need, yz, b, i, cnt, emit);
         else
-          build_range<false, false, BTPA>(qloc, q, mult, beg, end, bx0, by, bz, 0, yz, b, i, cnt, emit);
+          build_range<false, false, BTPA, PIPE>(qloc, q, mult, beg, end, bx0, by, bz, 0, yz, b, i, cnt, emit);
       }
       if (vhi > mx)  // through the +x face: the row's first cells, image shift +L
-        build_range<true, false, BTPA>(qloc, q, mult, xr[0], xr[vhi - mx], bxp, by, bz,
+        build_range<true, false, BTPA, PIPE>(qloc, q, mult, xr[0], xr[vhi - mx], bxp, by, bz,
                                        needed_strips(b.L[0], sy, sz), 2 | yz, b, i, cnt, emit);
     }
   }

@@ -533,7 +533,8 @@ __device__ __forceinline__ int ens_build_row(const Ens &e, int i) {
     auto emit = [&](int j, int k) {
       if (k < maxnb) e.nbr[(size_t)k * stride + i] = j;
     };
-    cnt = build_rows(box_of(e, rep), e.qloc, e.q, e.mult, e.xsub + rep.tab_off, e.cxyz[i], i, emit);
+    // without the load pipeline: it takes ke_build from 72 to 152 registers
+    cnt = build_rows<false, 1, false>(box_of(e, rep), e.qloc, e.q, e.mult, e.xsub + rep.tab_off, e.cxyz[i], i, emit);
   }
   e.nnbr[i] = min(cnt, maxnb);
   if (cnt > maxnb) {
