@@ -72,7 +72,8 @@ typedef struct {
   void *stream;             /* cudaStream_t to issue work on; NULL = handle-owned stream */
   int stage_atoms;          /* FP32-mixed: partner positions staged in shared memory per
                                128-atom block, at most this many atoms; 0 (default) = off,
-                               partners gathered from global memory; -1 = 2304 atoms */
+                               partners gathered from global memory; -1 = 2304 atoms.
+                               Steps with the staged pass run as graphs (step_mode). */
   int threads_per_atom;     /* FP32-mixed force pass: lanes per atom, 1, 2 or 4; every
                                choice gives bit-identical forces (fixed summation tree).
                                0 (default) = chosen by timing the three once per device
@@ -91,6 +92,11 @@ typedef struct {
                                atom from 16,384 atoms, 2 or 4 below); each stops at a step
                                that needs a rebuild, which a queued graph takes, and the
                                next launch follows without a host wait.  Same results. */
+  long long stage_wait_cycles; /* staged FP32-mixed pass (stage_atoms != 0): clock cycles a
+                               block waits for its stage copy before it reports
+                               MDG_ERR_TIMEOUT; it then still waits up to about a second
+                               for the copy to land before it exits.  0 (default): about a
+                               second.  A short limit tests the error path. */
 } mdg_params;
 
 enum { MDG_STEPS_AUTO = 0, MDG_STEPS_GRAPHS = 1, MDG_STEPS_PERSISTENT = 2 };

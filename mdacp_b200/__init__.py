@@ -85,6 +85,7 @@ class Params(ctypes.Structure):
         ("build_block", ctypes.c_int),
         ("build_threads_per_atom", ctypes.c_int),
         ("step_mode", ctypes.c_int),
+        ("stage_wait_cycles", ctypes.c_longlong),
     ]
 
 
@@ -280,7 +281,7 @@ class System:
                  thermostat=NVE, aimed_temperature=1.0, heatbath_tau=0.1, heatbath_gamma=0.1,
                  seed=0, buffer_length=0.3, check_list_length=500, max_neighbors=0, device=0,
                  stream=None, n_hint=None, stage_atoms=0, threads_per_atom=0, build_block=0,
-                 build_threads_per_atom=0, step_mode=0):
+                 build_threads_per_atom=0, step_mode=0, stage_wait_cycles=0):
         self.lib = load_library()
         p = Params()
         self.lib.mdg_default_params(ctypes.byref(p))
@@ -304,6 +305,7 @@ class System:
         p.build_block = int(build_block)
         p.build_threads_per_atom = int(build_threads_per_atom)
         p.step_mode = int(step_mode)
+        p.stage_wait_cycles = int(stage_wait_cycles)
         self.params = p
         h = _H()
         st = self.lib.mdg_create(ctypes.byref(p), ctypes.byref(h))

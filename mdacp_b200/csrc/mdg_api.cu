@@ -789,7 +789,9 @@ int persistent_grid(mdg_handle *h) {
 // Whether mdg_calculate runs the persistent pass: asked for, or (auto) when
 // one wave of resident blocks covers every atom's lanes.
 bool use_persistent(mdg_handle *h) {
-  if (!fused_step(h) || h->prm.step_mode == MDG_STEPS_GRAPHS) return false;
+  // the staged force pass (stage_atoms) runs as graph steps: the persistent
+  // pass gathers from global memory
+  if (!fused_step(h) || h->prm.step_mode == MDG_STEPS_GRAPHS || h->a.stage_cap > 0) return false;
   const int tpa = persistent_tpa(h);
   const int g = persistent_grid(h);
   if (g <= 0) return false;
@@ -923,7 +925,7 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   if (prm->capacity < 1 || prm->cutoff <= 0.0 || prm->buffer_length < 0.0 || prm->time_step <= 0.0 ||
       prm->check_list_length < 1 || (prm->precision != MDG_FP64 && prm->precision != MDG_FP32_MIXED) ||
       prm->thermostat < MDG_NVE || prm->thermostat > MDG_LANGEVIN || prm->stage_atoms < -1 ||
-      prm->stage_atoms > kStageMax ||
+      prm->stage_atoms > kStageMax || prm->stage_wait_cycles < 0 ||
       (prm->threads_per_atom != 0 && prm->threads_per_atom != 1 && prm->threads_per_atom != 2 &&
        prm->threads_per_atom != 4) ||
       (prm->build_block != 0 && prm->build_block != 64 && prm->build_block != 128 && prm->build_block != 256) ||
@@ -962,6 +964,7 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   b.rc2f = (float)b.rc2;
   b.c2x8f = (float)(b.c2 * 8.0);
   b.check_list_length = prm->check_list_length;
+  b.stage_wait = prm->stage_wait_cycles > 0 ? prm->stage_wait_cycles : kStageWaitCycles;
   h->ncell = b.ncell;
   h->cell_cap = b.ncell;
   h->cap = prm->capacity;

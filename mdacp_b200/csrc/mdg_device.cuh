@@ -70,6 +70,7 @@ struct Box {
   // and above (block nzl + 1).  A single domain has slab = 0, z0 = 0 and
   // nzl = ms[2].
   int slab, z0, nzl;
+  long long stage_wait;  // staged FP32 pass: cycles of the first wait for the stage copy
 };
 
 // Mutable device-side state of one handle.
@@ -1984,19 +1985,22 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
       : "memory");
 }
 
-// Waits for the mbarrier's phase `parity` to complete, for at most
-// `limit` clock cycles; false if it gave up.
+// Waits for the mbarrier's phase `parity` to complete, for at most `limit`
+// clock cycles; false if it gave up.  The test is the non-blocking
+// mbarrier.test_wait (PTX ISA), polled with a short sleep, so that a short
+// limit is kept to within a poll.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
   const long long t0 = clock64();
   while (true) {
     uint32_t done;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
         : "=r"(done)
         : "r"(smem_addr(bar)), "r"(parity)
         : "memory");
     if (done) return true;
     if (clock64() - t0 > limit) return false;
+    __nanosleep(20);
   }
 }
 
@@ -2007,8 +2011,9 @@ constexpr long long kStageWaitCycles = 2000000000ll;
 // from the block's stage (k_stage_plan) in dynamic shared memory, which one
 // thread fills with one bulk copy per plan range while the others wait on an
 // mbarrier.  Blocks without a plan (-1) gather from global memory.  If the
-// wait gives up (kStageWaitCycles), the block sets kErrTimeout, waits once
-// more for its copies in flight, and kicks no atom.
+// wait gives up (Box::stage_wait cycles, mdg_params.stage_wait_cycles), the
+// block sets kErrTimeout, waits once more (up to kStageWaitCycles) for its
+// copies in flight, and kicks no atom.
 template <int BLOCK, int MODE, int DRIFT>
 __global__ void __launch_bounds__(BLOCK) k_force_fp32_staged(Arrays a, Box b, int n, Thermo th, const int4 *qf,
                                                              int4 *qf_next) {
@@ -2061,7 +2066,7 @@ __global__ void __launch_bounds__(BLOCK) k_force_fp32_staged(Arrays a, Box b, in
         if (cnt > 0) bulk_load(pos + pr.w, qf + pr.z, (uint32_t)cnt * (uint32_t)sizeof(int4), &bar);
       }
     }
-    ok = mbar_wait(&bar, 0, kStageWaitCycles);
+    ok = mbar_wait(&bar, 0, b.stage_wait);
     if (!ok) {
       atomicOr(&a.st->error, kErrTimeout);
       mbar_wait(&bar, 0, kStageWaitCycles);

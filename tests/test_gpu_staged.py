@@ -112,3 +112,24 @@ def test_stage_size_is_checked():
     for bad in (-2, 12289):
         with pytest.raises(M.MdgError):
             M.System(st.L, cutoff=2.5, capacity=st.n, precision=M.FP32_MIXED, stage_atoms=bad)
+
+
+def test_stage_wait_that_runs_out_reports_timeout_and_the_device_stays_usable():
+    # a one-cycle limit on the first wait for the stage copy makes it give
+    # up (the copy takes microseconds): the block sets the timeout flag,
+    # waits for its copies with the normal limit before it exits, and the
+    # call returns MDG_ERR_TIMEOUT; a handle made afterwards steps normally
+    st = W.fcc_liquid(12, 0.8442, 1.0, seed=79, jitter=0.05, rc=2.5, dt=0.005)
+    s = M.System(st.L, cutoff=st.rc, time_step=st.dt, capacity=st.n, precision=M.FP32_MIXED,
+                 stage_atoms=-1, stage_wait_cycles=1)
+    s.set_state(st.q, st.v)
+    with pytest.raises(M.MdgError) as e:
+        s.calculate(5)
+    assert e.value.status == -8
+    s.close()
+    a, b = pair_of(st, -1)
+    a.calculate(20)
+    b.calculate(20)
+    assert_same(a, b)
+    with pytest.raises(M.MdgError):
+        M.System(st.L, cutoff=2.5, capacity=st.n, precision=M.FP32_MIXED, stage_atoms=-1, stage_wait_cycles=-1)
