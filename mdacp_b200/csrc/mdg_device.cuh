@@ -1101,19 +1101,17 @@ __device__ __forceinline__ int build_rows(const Box &b, const float4 *__restrict
   const int ms0 = b.ms[0], ms1 = b.ms[1], ms2 = b.ms[2];
   const float hi = b.sl2_hi;
   const int mx = ms0 * kXSub;
-  // sub-bins [vlo, vhi) of the virtual row of cells cx-1 .. cx+1 (unwrapped
-  // x) that can hold a partner: every bin that reaches [x_i - SL, x_i + SL];
-  // and the x bases of the three pieces (image shifts -L, 0, +L; prefilter
-  // x is global)
-  int vlo, vhi;
-  float bxm, bx0, bxp;
+  // x_i in sub-bins from the start of the virtual row of cells cx-1 .. cx+1
+  // (unwrapped x; bins of width cs/kXSub from each cell's lower face, as the
+  // trim table counts them), and the x bases of the three pieces (image
+  // shifts -L, 0, +L; prefilter x is global)
+  const int vbase = (cx - 1) * kXSub;
+  float ubin, per_binf, bxm, bx0, bxp;
   {
     const double qx = q[i].x;
     const double cs0 = b.cs[0], per_bin = kXSub / cs0;
-    vlo = (cx - 1) * kXSub + (int)floor((qx - (cx - 1) * cs0 - b.sl) * per_bin - 1e-6);
-    vhi = (cx + 1) * kXSub + (int)floor((qx - (cx + 1) * cs0 + b.sl) * per_bin + 1e-6) + 1;
-    vlo = max(vlo, (cx - 1) * kXSub);
-    vhi = min(vhi, (cx + 2) * kXSub);
+    ubin = (float)((qx - (cx - 1) * cs0) * per_bin);
+    per_binf = (float)per_bin;
     bxm = (float)(-b.L[0] - qx);
     bx0 = (float)(-qx);
     bxp = (float)(b.L[0] - qx);
@@ -1135,7 +1133,17 @@ __device__ __forceinline__ int build_rows(const Box &b, const float4 *__restrict
     }
     for (int dy = -1; dy <= 1; dy++) {
       const float gy = dy == 0 ? 0.f : (dy < 0 ? li.y : csy - li.y);
-      if (fmaf(gy, gy, gz * gz) > hi) continue;  // the whole row is out of reach
+      const float g2 = fmaf(gy, gy, gz * gz);
+      if (g2 > hi) continue;  // the whole row is out of reach
+      // sub-bins [vlo, vhi) of the row that can hold a partner: every bin
+      // that reaches x_i -/+ sqrt(hi - g2), the x reach left by the row's
+      // y-z gap g (hi is above SearchLength^2 by more than the FP32 error of
+      // g2; the bin edges get 1e-3 of a bin more)
+      const float reach = sqrtf(hi - g2) * per_binf;
+      int vlo = vbase + (int)floorf(ubin - reach - 1e-3f);
+      int vhi = vbase + (int)floorf(ubin + reach + 1e-3f) + 1;
+      vlo = max(vlo, vbase);
+      vhi = min(vhi, vbase + 3 * kXSub);
       int y = cy + dy, yc = 0;
       if (y < 0) { y += ms1; yc = 1; } else if (y >= ms1) { y -= ms1; yc = 2; }
       const double sy = yc == 1 ? -b.L[1] : (yc == 2 ? b.L[1] : 0.0);
