@@ -215,6 +215,9 @@ def main():
                     help="FP32-mixed NVE steps as CUDA graphs or one persistent launch (auto: by size)")
     ap.add_argument("--adjoint-launches", action="store_true",
                     help="c5 profiling: two 40-step gradient runs (checkpoints every 20 steps) and nothing else")
+    ap.add_argument("--tune-margins", action="store_true",
+                    help="c4: per-replica pairlist margins chosen by timing (mdacp_b200.margins) instead of "
+                         "the common BufferLength 0.3")
     ap.add_argument("--config", choices=["c2", "c1", "c3", "c4", "c5"], default="c2",
                     help="c2: 2.05M-atom liquid (headline); c1: 32k atoms rho 0.5; c3: 1M-atom Langevin slab; "
                          "c4: 256-replica ensemble; c5: adjoint gradients of a 32k-atom trajectory")
@@ -689,8 +692,13 @@ def main_ensemble(args, ws, rank, local):
     ntot_all = sum(r.n for r in all_reps)
     ntot = sum(r.n for r in reps)
     mdn = args.md_steps_per_step
+    margins, tuning = None, None
+    if args.tune_margins:
+        # outside the timed region: trial ensembles of this rank's replicas
+        margins, tuning = M.margins.tune_margins([(r.q, r.v, r.L) for r in reps], cutoff=2.5, time_step=0.005,
+                                                 precision=M.FP32_MIXED, device=local)
     ens = M.Ensemble([(r.q, r.v, r.L) for r in reps], cutoff=2.5, time_step=0.005, precision=M.FP32_MIXED,
-                     device=local)
+                     device=local, buffer_lengths=margins)
     if args.eager:
         ens.set_graph_mode(False)
     for _ in range(args.warmup):
@@ -737,12 +745,14 @@ def main_ensemble(args, ws, rank, local):
     # (replicas narrower than three search lengths on an axis have no
     # single-system cell grid and are left out of the loop)
     loop_steps = max(20, mdn // 5)
-    sl = 2.5 + 0.3
-    looped = [r for r in reps if min(int(x / sl) for x in r.L) >= 3] if ws == 1 else []
-    loop_n = sum(r.n for r in looped)
+    rep_margin = list(margins) if margins is not None else [0.3] * len(reps)
+    looped = [(r, m) for r, m in zip(reps, rep_margin) if min(int(x / (2.5 + m)) for x in r.L) >= 3] \
+        if ws == 1 else []
+    loop_n = sum(r.n for r, _ in looped)
     systems = []
-    for r in looped:
-        sy = M.System(r.L, cutoff=2.5, time_step=0.005, capacity=r.n, precision=M.FP32_MIXED, device=local)
+    for r, m in looped:
+        sy = M.System(r.L, cutoff=2.5, time_step=0.005, capacity=r.n, precision=M.FP32_MIXED, device=local,
+                      buffer_length=m)
         sy.set_state(r.q, r.v)
         sy.calculate(20)  # first build + graph capture outside the timing
         systems.append(sy)
@@ -760,8 +770,13 @@ def main_ensemble(args, ws, rank, local):
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"256 replicas, {ntot_all} atoms in total, N 500-20000, rho 0.3-0.9, T 0.7-1.5, "
-                               "jittered FCC, rc 2.5, search length 2.8, dt 0.005, NVE, FP32-mixed",
+                               f"jittered FCC, rc 2.5, search length "
+                               f"{'2.5 + tuned margin' if margins is not None else '2.8'}, dt 0.005, NVE, FP32-mixed",
                    "md_steps_per_step": mdn, "replicas": len(all_reps), "atoms": ntot_all,
+                   "buffer_length": ("per replica, chosen by timing (rank 0's share: min %.3f, median %.3f, "
+                                     "max %.3f)" % (float(np.min(margins)), float(np.median(margins)),
+                                                    float(np.max(margins)))) if margins is not None else 0.3,
+                   "margin_tuning": tuning,
                    "rebuilds_per_replica_mean": float(np.mean(rb_all)),
                    "rebuilds_per_replica_max": float(np.max(rb_all)),
                    "energy_per_atom_mean": float(np.mean((per_rep[:, 1] + per_rep[:, 2]) /

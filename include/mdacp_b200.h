@@ -78,7 +78,7 @@ typedef struct {
                                choice gives bit-identical forces (fixed summation tree).
                                0 (default) = chosen by timing the three once per device
                                and problem shape, at the first step */
-  int build_block;          /* list build: threads per block, 64, 128 or 256; 0
+  int build_block;          /* list build: threads per block, 32, 64, 128 or 256; 0
                                (default) = chosen by timing, as threads_per_atom */
   int build_threads_per_atom; /* list build: lanes per atom, 1, 2, 4 or 8 (the rows are the
                                same for every choice); 0 (default) = chosen by timing
@@ -277,6 +277,10 @@ typedef struct mdg_ensemble mdg_ensemble;
 typedef struct {
   int n;          /* atoms */
   double L[3];    /* box; every length must exceed 2 x SearchLength */
+  double buffer_length; /* > 0: this replica's BufferLength (its SearchLength is
+                           cutoff + this, its skin budget starts at this); 0: the
+                           common buffer_length.  A replica evolves as a single
+                           system with the same buffer_length. */
 } mdg_replica;
 /* common: cutoff, buffer_length, time_step, precision, check_list_length,
    device (capacity, thermostat and stream are not used). */

@@ -158,7 +158,7 @@ SNAPSHOT_CDVIEW, SNAPSHOT_CONFIGURATION = 0, 1
 class Replica(ctypes.Structure):
     """``mdg_replica`` (include/mdacp_b200.h)."""
 
-    _fields_ = [("n", ctypes.c_int), ("L", ctypes.c_double * 3)]
+    _fields_ = [("n", ctypes.c_int), ("L", ctypes.c_double * 3), ("buffer_length", ctypes.c_double)]
 
 
 # name -> (restype, argtypes)
@@ -644,10 +644,12 @@ def partition_replicas(boxes, nranks, search_length=2.8):
 
 class Ensemble:
     """Independent periodic replicas advanced together (mdg_ensemble_*).
-    ``states`` is a list of (q, v, L) per replica."""
+    ``states`` is a list of (q, v, L) per replica; ``buffer_lengths``
+    (optional, one per replica, 0 = ``buffer_length``) gives replicas their
+    own BufferLength (for example from :func:`choose_margins`)."""
 
     def __init__(self, states, cutoff=2.5, time_step=0.005, precision=FP64, buffer_length=0.3,
-                 check_list_length=500, device=0, threads_per_atom=0):
+                 check_list_length=500, device=0, threads_per_atom=0, buffer_lengths=None):
         self.lib = load_library()
         p = Params()
         self.lib.mdg_default_params(ctypes.byref(p))
@@ -661,9 +663,12 @@ class Ensemble:
         self.nrep = len(states)
         reps = (Replica * self.nrep)()
         self.sizes = []
+        if buffer_lengths is not None and len(buffer_lengths) != self.nrep:
+            raise ValueError("one buffer length per replica")
         for k, (q, v, L) in enumerate(states):
             reps[k].n = int(q.shape[0])
             reps[k].L[:] = [float(x) for x in L]
+            reps[k].buffer_length = 0.0 if buffer_lengths is None else float(buffer_lengths[k])
             self.sizes.append(int(q.shape[0]))
         self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
         h = _H()
@@ -748,3 +753,6 @@ class Ensemble:
         s = np.empty(self.nrep, dtype=np.int64)
         self._check(self.lib.mdg_ensemble_rebuilds(self.h, r.ctypes.data_as(_I64P), s.ctypes.data_as(_I64P)))
         return r, s
+
+
+from . import margins  # noqa: E402  (per-replica margin tuner; imports this package lazily)

@@ -40,6 +40,10 @@ struct Rep {
   int ncell, cell_off, atom_off, n;
   long long tab_off;  // first entry of the replica's rows in the trim table
   int small;  // all-pairs search (fewer than 3 cells along an axis)
+  // the replica's BufferLength, SearchLength = cut-off + it, and the FP32
+  // prefilter band around SearchLength^2
+  double buffer_length, sl, sl2;
+  float sl2_lo, sl2_hi;
 };
 
 struct RepStatus {
@@ -82,8 +86,8 @@ struct Ens {
   double *sums;  // nrep x 3 observer sums
   WorkList wd, wb;  // skin-check and rebuild work lists
   int stride, maxnb, nrep, ntot, cll;
-  double rc2, sl, sl2, c0, c2, dt, buffer_length;
-  float rc2f, c2x8f, sl2_lo, sl2_hi;
+  double rc2, c0, c2, dt;
+  float rc2f, c2x8f;
 };
 
 // Box of a replica in the single-system kernels' layout.
@@ -98,18 +102,18 @@ __device__ __forceinline__ Box box_of(const Ens &e, const Rep &r) {
     b.fix_scale[d] = r.fix_scale[d];
   }
   b.ncell = r.ncell;
-  b.sl = e.sl;
-  b.sl2 = e.sl2;
+  b.sl = r.sl;
+  b.sl2 = r.sl2;
   b.rc2 = e.rc2;
   b.c0 = e.c0;
   b.c2 = e.c2;
   b.dt = e.dt;
-  b.buffer_length = e.buffer_length;
+  b.buffer_length = r.buffer_length;
   b.rc2f = e.rc2f;
   b.c2x8f = e.c2x8f;
   b.check_list_length = e.cll;
-  b.sl2_lo = e.sl2_lo;
-  b.sl2_hi = e.sl2_hi;
+  b.sl2_lo = r.sl2_lo;
+  b.sl2_hi = r.sl2_hi;
   b.slab = 0;
   b.z0 = 0;
   b.nzl = r.ms[2];
@@ -235,7 +239,7 @@ __global__ void ke_expiry(Ens e, cudaGraphConditionalHandle h_disp, int in_graph
       } else {
         if (st.budget > 0.0) {
           const double vmax = sqrt(__longlong_as_double((long long)st.vmax2_bits));
-          if (skin_cost(vmax, e.dt) > e.buffer_length) atomicOr(e.error, kErrTooFast);
+          if (skin_cost(vmax, e.dt) > e.rep[r].buffer_length) atomicOr(e.error, kErrTooFast);
           else st.budget = dsub(st.budget, skin_cost(vmax, e.dt));
         }
         if (st.budget < 0.0) {
@@ -286,7 +290,7 @@ __global__ void __launch_bounds__(kEB) ke_disp_collect(Ens e) {
     int r;
     const int i = work_atom(e, e.wd, g, &r);
     RepStatus &st = e.rs[r];
-    const double c = e.buffer_length - sqrt(__longlong_as_double((long long)st.dr2max_bits));
+    const double c = e.rep[r].buffer_length - sqrt(__longlong_as_double((long long)st.dr2max_bits));
     const double c_d2 = c * c;
     for_each_copy(ens_view(e), e.rep[r].L, i, e.lag, [&](int code, double d2) {
       if (d2 > c_d2) {
@@ -315,7 +319,7 @@ __global__ void __launch_bounds__(256) ke_disp_pairs(Ens e) {
     if (threadIdx.x == 0) found = 1;
   } else {
     const int l = min(st.cand_n, e.cll);
-    candidate_pair_test<256>(ens_view(e), rep.L, e.cand + (size_t)r * e.cll, l, e.lag, e.sl2, e.rc2, blockIdx.y,
+    candidate_pair_test<256>(ens_view(e), rep.L, e.cand + (size_t)r * e.cll, l, e.lag, rep.sl2, e.rc2, blockIdx.y,
                              gridDim.y, sm, &found);
   }
   __syncthreads();
@@ -525,7 +529,7 @@ __device__ __forceinline__ int ens_build_row(const Ens &e, int i) {
       const double sz = tz > rep.hL[2] ? -rep.L[2] : (tz < -rep.hL[2] ? rep.L[2] : 0.0);
       const int need = needed_strips(sx, sy, sz);
       if (need && (e.mult[j] & need) != need) continue;
-      if (!within_search_exact(qi, qj, sx, sy, sz, e.sl2)) continue;
+      if (!within_search_exact(qi, qj, sx, sy, sz, rep.sl2)) continue;
       if (cnt < maxnb) e.nbr[(size_t)cnt * stride + i] = j;
       cnt++;
     }
@@ -561,7 +565,7 @@ __global__ void ke_build_done(Ens e) {
   for (int r = threadIdx.x; r < e.nrep; r += blockDim.x) {
     RepStatus &st = e.rs[r];
     if (!st.build || *e.error) continue;
-    st.budget = e.buffer_length;
+    st.budget = e.rep[r].buffer_length;
     st.list_stale = 0;
     st.rebuilds++;
   }
@@ -1058,7 +1062,6 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MDG_ERR_NO_DEVICE;
   if (prm->device < 0 || prm->device >= ndev) return MDG_ERR_INVALID_ARGUMENT;
   if (cudaSetDevice(prm->device) != cudaSuccess) return MDG_ERR_CUDA;
-  const double SL = prm->cutoff + prm->buffer_length;
   mdg_ensemble *x = new mdg_ensemble();
   x->prm = *prm;
   if (prm->threads_per_atom != 0 && prm->threads_per_atom != 1 && prm->threads_per_atom != 2 &&
@@ -1073,10 +1076,15 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
   for (int r = 0; r < nrep; r++) {
     Rep &rp = x->reps[r];
     memset(&rp, 0, sizeof rp);
-    if (replicas[r].n < 0) {
+    if (replicas[r].n < 0 || !(replicas[r].buffer_length >= 0.0) || !std::isfinite(replicas[r].buffer_length)) {
       delete x;
       return MDG_ERR_INVALID_ARGUMENT;
     }
+    rp.buffer_length = replicas[r].buffer_length > 0.0 ? replicas[r].buffer_length : prm->buffer_length;
+    const double SL = prm->cutoff + rp.buffer_length;
+    rp.sl = SL;
+    rp.sl2 = SL * SL;
+    prefilter_band(rp.sl2, SL, replicas[r].L[0], &rp.sl2_lo, &rp.sl2_hi);
     int small = 0;
     for (int d = 0; d < 3; d++) {
       const double L = replicas[r].L[d];
@@ -1119,8 +1127,6 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
   e.ntot = (int)atoms;
   e.cll = prm->check_list_length;
   e.stride = (e.ntot + 31) / 32 * 32;
-  e.sl = SL;
-  e.sl2 = SL * SL;
   e.rc2 = prm->cutoff * prm->cutoff;
   {
     const double s2 = 1.0 / (prm->cutoff * prm->cutoff);
@@ -1129,15 +1135,9 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
     e.c0 = -s12 + s6 - e.c2 / s2;
   }
   e.dt = prm->time_step;
-  e.buffer_length = prm->buffer_length;
   e.lag = 0.5 * prm->time_step;  // NVE: ghosts refreshed before the last half drift
   e.rc2f = (float)e.rc2;
   e.c2x8f = (float)(e.c2 * 8.0);
-  {
-    double lx = 0.0;
-    for (int r = 0; r < nrep; r++) lx = std::max(lx, x->reps[r].L[0]);
-    prefilter_band(e.sl2, SL, lx, &e.sl2_lo, &e.sl2_hi);
-  }
   x->ncell_tot = cells;
   const size_t n = (size_t)std::max<long long>(atoms, 1);
   cudaError_t err = cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking);
@@ -1244,7 +1244,7 @@ mdg_status mdg_ensemble_set_state(mdg_ensemble *x, const double *q4, const doubl
     for (int k = 0; k < rp.n; k++) ids[rp.atom_off + k] = k;  // upload index within the replica
     // neighbour-row capacity from the replica's density
     const double vol = rp.L[0] * rp.L[1] * rp.L[2];
-    const double sphere = 4.0 / 3.0 * M_PI * e.sl * e.sl * e.sl;
+    const double sphere = 4.0 / 3.0 * M_PI * rp.sl * rp.sl * rp.sl;
     maxnb = std::max(maxnb, std::min(rp.n, (int)std::ceil(1.6 * (rp.n / vol) * sphere + 32.0)));
   }
   ECUDA(cudaMemcpyAsync(e.ids, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice, x->stream));
@@ -1253,10 +1253,11 @@ mdg_status mdg_ensemble_set_state(mdg_ensemble *x, const double *q4, const doubl
   std::vector<RepStatus> rs(e.nrep);
   ECUDA(cudaMemcpyAsync(rs.data(), e.rs, sizeof(RepStatus) * e.nrep, cudaMemcpyDeviceToHost, x->stream));
   ECUDA(cudaStreamSynchronize(x->stream));
-  for (auto &s : rs) {
+  for (int k = 0; k < e.nrep; k++) {
+    RepStatus &s = rs[k];
     s.list_stale = 1;
     s.vmax2_bits = 0;
-    s.budget = e.buffer_length;
+    s.budget = x->reps[k].buffer_length;
     s.build = s.want_build = s.disp = 0;
   }
   const int zero = 0;

@@ -50,6 +50,45 @@ def test_ensemble_bit_identical_to_single(precision):
         s.close()
 
 
+def test_per_replica_margins_match_single_systems_with_that_margin():
+    # each replica's own BufferLength (0 = the common 0.3): its search
+    # length, cell grid, skin budget and rebuild schedule are those of a
+    # single handle made with that buffer length, bit for bit
+    reps = replicas()
+    margins = [0.75, 0.2, 0.5, 0.0]  # every replica keeps three or more cells per axis
+    ens = M.Ensemble([(r.q, r.v, r.L) for r in reps], cutoff=2.5, time_step=0.005, precision=M.FP32_MIXED,
+                     buffer_lengths=margins)
+    ens.calculate(80)
+    got = ens.states_by_id()
+    rb, _ = ens.rebuilds()
+    for k, r in enumerate(reps):
+        s = M.System(r.L, cutoff=2.5, time_step=0.005, capacity=r.n, precision=M.FP32_MIXED,
+                     buffer_length=margins[k] or 0.3)
+        s.set_state(r.q, r.v)
+        s.calculate(80)
+        q, v = s.state_by_id()
+        assert np.array_equal(got[k][0], q), f"replica {k} positions"
+        assert np.array_equal(got[k][1], v), f"replica {k} velocities"
+        assert rb[k] == s.info()["rebuilds"], f"replica {k} rebuilds"
+        s.close()
+    ens.close()
+    # a margin is checked against the replica's own box
+    with pytest.raises(M.MdgError) as e:
+        M.Ensemble([(reps[3].q, reps[3].v, reps[3].L)], cutoff=2.5, buffer_lengths=[reps[3].L[0] / 2.0])
+    assert e.value.status == -7
+    with pytest.raises(M.MdgError):
+        M.Ensemble([(reps[0].q, reps[0].v, reps[0].L)], cutoff=2.5, buffer_lengths=[-0.1])
+
+
+def test_margin_tuner_runs_and_keeps_the_fastest_trial():
+    reps = replicas()
+    margins, report = M.margins.tune_margins([(r.q, r.v, r.L) for r in reps], cutoff=2.5, time_step=0.005,
+                                              warm_steps=20, trial_steps=40, costs=(6.0,))
+    assert len(margins) == len(reps) and np.all(margins >= 0.1)
+    times = [t["ms_per_step"] for t in report["trials"]]
+    assert len(times) == 2 and report["chosen_ms_per_step"] == min(times)
+
+
 def test_small_replica_all_pairs_matches_oracle():
     # 500 atoms at rho 0.9: L = 8.22 < 3 x 2.8, two cells per axis
     small = W.fcc_liquid(5, 0.9, 1.0, seed=65, jitter=0.05, rc=2.5, dt=0.005)
