@@ -78,7 +78,7 @@ typedef struct {
                                choice gives bit-identical forces (fixed summation tree).
                                0 (default) = chosen by timing the three once per device
                                and problem shape, at the first step */
-  int build_block;          /* list build: threads per block, 32, 64, 128 or 256; 0
+  int build_block;          /* list build: threads per block, 64, 128 or 256; 0
                                (default) = chosen by timing, as threads_per_atom */
   int build_threads_per_atom; /* list build: lanes per atom, 1, 2, 4 or 8 (the rows are the
                                same for every choice); 0 (default) = chosen by timing
