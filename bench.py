@@ -208,7 +208,8 @@ def main():
     ap.add_argument("--eager", action="store_true",
                     help="launch every kernel from the host instead of CUDA graphs (for profilers)")
     ap.add_argument("--threads-per-atom", type=int, default=0,
-                    help="FP32-mixed force pass lanes per atom (0: tuned at the first step)")
+                    help="FP32-mixed force pass lanes per atom (0: tuned at the first step); with "
+                         "--config c5 --adjoint-launches the adjoint pair kernels' lanes (1, 2, 4, 8)")
     ap.add_argument("--build-block", type=int, default=0, help="list build threads per block (0: tuned)")
     ap.add_argument("--build-lanes", type=int, default=0, help="list build lanes per atom (0: tuned)")
     ap.add_argument("--step-mode", choices=["auto", "graphs", "persistent"], default="auto",
@@ -581,9 +582,11 @@ def main_adjoint(args, ws, rank, local):
     torch.cuda.set_device(local)
     st = W.config_c5(seed=55 + rank)
     if args.adjoint_launches:
-        # the sequence of profiles/adjoint_lj32000_launches.md: the
-        # lanes-per-atom autotuner and warm-up, then one 40-step gradient run
-        kw = dict(steps=40, checkpoint_every=20, time_step=st.dt, device=local)
+        # the sequence of profiles/adjoint_lj32000_launches.md: a warm-up
+        # run (with the lanes-per-atom autotuner unless --threads-per-atom
+        # pins the lanes), then one 40-step gradient run
+        kw = dict(steps=40, checkpoint_every=20, time_step=st.dt, device=local,
+                  threads_per_atom=args.threads_per_atom)
         A.trajectory_gradients(st.q, st.v, st.L, **kw)
         t0 = time.perf_counter()
         A.trajectory_gradients(st.q, st.v, st.L, **kw)

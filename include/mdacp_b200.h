@@ -436,7 +436,11 @@ mdg_status mdg_external_state(mdg_handle *h, double *position, double *impulse);
  * reference's smoothed phi (src/variables.cc:16-33) and the cut-off in units
  * of sigma; steps as MDManager::Calculate (NVE, src/mdmanager.cc:153-186), in
  * FP64.  Loss L = 1/(steps n) sum over the steps' end states of
- * [PE + sum over pairs g((r-lo)/w) g((hi-r)/w)], g the logistic function. */
+ * [PE + sum over pairs g((r-lo)/w) g((hi-r)/w)], g the logistic function.
+ * Pairs come from a Verlet list of search length cutoff + 0.3 sigma (less in
+ * boxes narrower than three such lengths), rebuilt when an atom has moved
+ * half the skin; its rows are in ascending partner order, so the sums are a
+ * function of the positions alone (and of threads_per_atom). */
 typedef struct mdg_adjoint_params {
   double L[3];
   double cutoff;          /* in units of sigma (CUTOFF_LENGTH, include/mdconfig.h:31) */
@@ -454,7 +458,9 @@ void mdg_adjoint_default_params(mdg_adjoint_params *p);
 /* q0, v0: n x 3 doubles.  loss is required; with all three gradient
  * pointers NULL only the forward pass runs.  dloss_dq0: n x 3 doubles.
  * Allocates its device memory per call (checkpoints: 2 x 32 B per atom per
- * checkpoint). */
+ * checkpoint; the list: 4 B per row entry, rows of up to 1024 entries).
+ * MDG_ERR_CAPACITY if a row outgrows its capacity (three times the mean
+ * density's count within the search length, plus 64). */
 mdg_status mdg_adjoint_run(const mdg_adjoint_params *p, const double *q0, const double *v0, int n, double *loss,
                            double *dloss_deps, double *dloss_dsigma, double *dloss_dq0);
 

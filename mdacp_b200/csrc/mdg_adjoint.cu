@@ -24,11 +24,14 @@
 // k steps in the forward pass; each k-step segment is recomputed forward
 // (keeping q_h and v') before its reverse sweep.
 //
-// Pairs are found through a cell grid rebuilt for every evaluation (cells at
-// least r_c = s_c sigma wide, >= 3 per axis, atoms in each cell ordered by
-// index), so every sum is deterministic and no skin bookkeeping is needed.
-// This component has no counterpart in the reference, which has no
-// gradients.
+// Pairs come from a Verlet list of search length r_c + skin (r_c = s_c
+// sigma; skin 0.3 sigma, less where the box is narrow), built from a cell
+// grid (cells at least r_c + skin wide, >= 3 per axis, atoms in each cell
+// ordered by index, rows in cell-walk order, so every sum is deterministic).
+// Before each evaluation every atom's displacement from the list's build
+// positions is checked; the list is rebuilt when one exceeds skin/2, which
+// keeps every pair within r_c in the rows.  This component has no
+// counterpart in the reference, which has no gradients.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -59,6 +62,13 @@ struct Grid {
   const int *start;   // ncell + 1
   const int *perm;    // atoms in cell order
   const double4 *qs;  // their positions in the same order (made with the grid)
+};
+
+// The Verlet list: row of atom i = entries nbr[k * n + i], k < cnt[i].
+struct Rows {
+  const int *nbr;
+  const int *cnt;
+  double inv_L[3], L[3];
 };
 
 // phi(s) and its first two derivatives; one division (1/s).
@@ -104,31 +114,70 @@ __device__ __forceinline__ int cell_of(const double4 &q, const Grid &g) {
   return (cz * g.ms[1] + cy) * g.ms[0] + cx;
 }
 
-// Calls f(j, d, r) for every partner j != i with r < r_c, d = minimum image of
-// q_i - q_j, over the 27 cells around i's, each in index order (partner
-// positions read from the grid's cell-ordered copy).  TPA lanes
-// share one atom: lane `sub` takes cells sub, sub + TPA, ... of the 27 (the
-// caller combines the lanes' sums with group_sum).
+// Calls f(j, d, r) for every partner j of i's row with r < r_c, d = minimum
+// image of q_i - q_j, in row order (ascending j).  Rows hold every pair
+// within r_c and more, in ascending j, so the pairs within r_c and their
+// order are a function of q alone, whichever build the row comes from.
+// TPA lanes share one atom: they test TPA entries at a time, number the
+// pairs within r_c in row order, and lane `sub` takes pairs sub, sub + TPA,
+// ... of that numbering (shuffled to it from the lane that tested them); the
+// caller combines the lanes' sums with group_sum.  All TPA lanes of the atom
+// call together.
 template <int TPA, class F>
-__device__ __forceinline__ void for_pairs(const double4 *q, const Grid &g, const Pot &p, int i, int sub, F f) {
+__device__ __forceinline__ void for_pairs(const double4 *q, const Rows &w, const Pot &p, int i, int sub, int n,
+                                          F f) {
   const double4 qi = q[i];
-  const int cx = cell_axis(qi.x, g.L[0], g.inv_cs[0], g.ms[0]);
-  const int cy = cell_axis(qi.y, g.L[1], g.inv_cs[1], g.ms[1]);
-  const int cz = cell_axis(qi.z, g.L[2], g.inv_cs[2], g.ms[2]);
-  for (int nbh = sub; nbh < 27; nbh += TPA) {
-    const int z = (cz + nbh / 9 - 1 + g.ms[2]) % g.ms[2];
-    const int y = (cy + (nbh / 3) % 3 - 1 + g.ms[1]) % g.ms[1];
-    const int x = (cx + nbh % 3 - 1 + g.ms[0]) % g.ms[0];
-    const int c = (z * g.ms[1] + y) * g.ms[0] + x;
-    for (int k = g.start[c]; k < g.start[c + 1]; k++) {
-      const int j = g.perm[k];
-      if (j == i) continue;
-      const double4 qj = g.qs[k];
-      double d[3] = {qi.x - qj.x, qi.y - qj.y, qi.z - qj.z};
-      for (int a = 0; a < 3; a++) d[a] -= g.L[a] * rint(d[a] * g.inv_L[a]);
-      const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  const int m = w.cnt[i];
+  auto pair_of = [&](int k, int &j, double (&d)[3]) {
+    j = w.nbr[(size_t)k * n + i];
+    const double4 qj = q[j];
+    d[0] = qi.x - qj.x;
+    d[1] = qi.y - qj.y;
+    d[2] = qi.z - qj.z;
+    for (int a = 0; a < 3; a++) d[a] -= w.L[a] * rint(d[a] * w.inv_L[a]);
+    return d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  };
+  if (TPA == 1) {
+    for (int k = 0; k < m; k++) {
+      int j;
+      double d[3];
+      const double r2 = pair_of(k, j, d);
       if (r2 < p.rc2) f(j, d, sqrt(r2));
     }
+    return;
+  }
+  const int lane = threadIdx.x & 31, first = lane & ~(TPA - 1);
+  const unsigned gmask = (TPA == 32) ? 0xffffffffu : (((1u << TPA) - 1u) << first);
+  int before = 0;  // pairs within r_c in the entries already tested
+  for (int k0 = 0; k0 < m; k0 += TPA) {
+    int j = 0;
+    double d[3] = {0.0, 0.0, 0.0}, r2 = 0.0;
+    bool in = false;
+    if (k0 + sub < m) {
+      r2 = pair_of(k0 + sub, j, d);
+      in = r2 < p.rc2;
+    }
+    const unsigned bal = (__ballot_sync(gmask, in) >> first) & ((1u << TPA) - 1u);
+    const int cnt = __popc(bal);
+    // this lane's pair of the batch: number r of the batch's pairs, the one
+    // with overall number == sub (mod TPA)
+    const int r = (sub - before % TPA + TPA) % TPA;
+    int src = 0;
+#pragma unroll
+    for (int b = 0, c = 0; b < TPA; b++) {
+      if ((bal >> b) & 1u) {
+        if (c == r) src = b;
+        c++;
+      }
+    }
+    const int jj = __shfl_sync(gmask, j, first + src);
+    double dd[3];
+    dd[0] = __shfl_sync(gmask, d[0], first + src);
+    dd[1] = __shfl_sync(gmask, d[1], first + src);
+    dd[2] = __shfl_sync(gmask, d[2], first + src);
+    const double rr = __shfl_sync(gmask, r2, first + src);
+    if (r < cnt) f(jj, dd, sqrt(rr));
+    before += cnt;
   }
 }
 
@@ -161,16 +210,23 @@ __device__ __forceinline__ void block_sums(double (&v)[NS], double *part) {
 }
 
 // ------------------------------------------------------------------ cells
-__global__ void a_count(const double4 *q, int n, Grid g, int *cell, int *count) {
+// The grid kernels run only when the list is to be rebuilt (*want != 0).
+__global__ void a_clear(int *count, int *fill, int ncell, const int *want) {
+  if (!*want) return;
+  for (int c = blockIdx.x * kAB + threadIdx.x; c < ncell; c += gridDim.x * kAB) count[c] = fill[c] = 0;
+}
+
+__global__ void a_count(const double4 *q, int n, Grid g, int *cell, int *count, const int *want) {
   const int i = blockIdx.x * kAB + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || !*want) return;
   const int c = cell_of(q[i], g);
   cell[i] = c;
   atomicAdd(&count[c], 1);
 }
 
 // exclusive scan of count into start (one block, ncell of any size)
-__global__ void a_scan(const int *count, int *start, int ncell) {
+__global__ void a_scan(const int *count, int *start, int ncell, const int *want) {
+  if (!*want) return;
   __shared__ int part[1024];
   const int t = threadIdx.x;
   const int chunk = (ncell + 1023) / 1024;
@@ -193,9 +249,9 @@ __global__ void a_scan(const int *count, int *start, int ncell) {
   if (t == 1023) start[ncell] = part[t];
 }
 
-__global__ void a_fill(int n, const int *cell, const int *start, int *fill, int *perm) {
+__global__ void a_fill(int n, const int *cell, const int *start, int *fill, int *perm, const int *want) {
   const int i = blockIdx.x * kAB + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || !*want) return;
   const int c = cell[i];
   perm[start[c] + atomicAdd(&fill[c], 1)] = i;
 }
@@ -203,10 +259,10 @@ __global__ void a_fill(int n, const int *cell, const int *start, int *fill, int 
 // Orders every cell by atom index, one warp per cell: each entry's new
 // place is the count of smaller indices in the cell (indices are distinct).
 // perm_in is the fill order, perm_out the sorted one.
-__global__ void a_sort(int ncell, const int *start, const int *perm_in, int *perm_out) {
+__global__ void a_sort(int ncell, const int *start, const int *perm_in, int *perm_out, const int *want) {
   const int c = (blockIdx.x * kAB + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (c >= ncell) return;
+  if (c >= ncell || !*want) return;
   const int b = start[c], cnt = start[c + 1] - b;
   for (int base = 0; base < cnt; base += 32) {
     const int me = base + lane;
@@ -221,19 +277,209 @@ __global__ void a_sort(int ncell, const int *start, const int *perm_in, int *per
 }
 
 // Positions in cell order for the pair kernels.
-__global__ void a_gather(const double4 *x, const int *perm, double4 *xs, int n) {
+__global__ void a_gather(const double4 *x, const int *perm, double4 *xs, int n, const int *want) {
   const int k = blockIdx.x * kAB + threadIdx.x;
-  if (k < n) xs[k] = x[perm[k]];
+  if (k < n && *want) xs[k] = x[perm[k]];
+}
+
+// The whole grid (clear, count, scan, fill, per-cell index order, gather)
+// in one block of 1024 threads, for up to kGrid1Atoms atoms.
+constexpr int kGrid1Atoms = 262144;
+__global__ void __launch_bounds__(1024) a_grid1(const double4 *x, int n, Grid g, int ncell, int *cell, int *count,
+                                                int *start, int *fill, int *perm_fill, int *perm, double4 *qs,
+                                                const int *want) {
+  if (!*want) return;
+  __shared__ int part[1024];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  for (int c = t; c < ncell; c += 1024) count[c] = fill[c] = 0;
+  __syncthreads();
+  for (int i = t; i < n; i += 1024) {
+    const int c = cell_of(x[i], g);
+    cell[i] = c;
+    atomicAdd(&count[c], 1);
+  }
+  __syncthreads();
+  {  // exclusive scan of count into start, 1024 chunks
+    const int chunk = (ncell + 1023) / 1024;
+    const int beg = min(t * chunk, ncell), end = min(beg + chunk, ncell);
+    int sum = 0;
+    for (int c = beg; c < end; c++) sum += count[c];
+    part[t] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+      const int v = t >= o ? part[t - o] : 0;
+      __syncthreads();
+      part[t] += v;
+      __syncthreads();
+    }
+    int run = part[t] - sum;
+    for (int c = beg; c < end; c++) {
+      start[c] = run;
+      run += count[c];
+    }
+    if (t == 1023) start[ncell] = part[t];
+  }
+  __syncthreads();
+  for (int i = t; i < n; i += 1024) {
+    const int c = cell[i];
+    perm_fill[start[c] + atomicAdd(&fill[c], 1)] = i;
+  }
+  __syncthreads();
+  for (int c = warp; c < ncell; c += 32) {  // index order inside each cell (as a_sort)
+    const int b = start[c], cnt = start[c + 1] - b;
+    for (int base = 0; base < cnt; base += 32) {
+      const int me = base + lane;
+      const int key = me < cnt ? perm_fill[b + me] : 0x7fffffff;
+      int rank = 0;
+      for (int ob = 0; ob < cnt; ob += 32) {
+        const int okey = ob + lane < cnt ? perm_fill[b + ob + lane] : 0x7fffffff;
+        for (int k = 0; k < 32; k++) rank += (ob + k < cnt) && (__shfl_sync(0xffffffffu, okey, k) < key);
+      }
+      if (me < cnt) perm[b + rank] = key;
+    }
+  }
+  __syncthreads();
+  for (int k = t; k < n; k += 1024) qs[k] = x[perm[k]];
+}
+
+// ---------------------------------------------------------- Verlet list
+// flag[0] = 1 if some atom moved more than skin/2 from the list's build
+// positions qb (minimum image); flag[0] starts at 1 for the first build.
+__global__ void a_check(const double4 *x, const double4 *qb, int n, Rows w, double half_skin2, int *flag) {
+  const int i = blockIdx.x * kAB + threadIdx.x;
+  if (i >= n) return;
+  const double4 a = x[i], b = qb[i];
+  double d[3] = {a.x - b.x, a.y - b.y, a.z - b.z};
+  for (int k = 0; k < 3; k++) d[k] -= w.L[k] * rint(d[k] * w.inv_L[k]);
+  if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] > half_skin2) atomicOr(flag, 1);
+}
+
+// Ascending sort of the 32 E values of a warp, v[e] = element e * 32 + lane
+// (bitonic network, fully unrolled).
+template <int E>
+__device__ __forceinline__ void warp_sort_asc(int (&v)[E], int lane) {
+  constexpr int N = 32 * E;
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        if (j < 32) {  // partner in lane ^ j, same e
+          const int g = e * 32 + lane;
+          const int o = __shfl_xor_sync(0xffffffffu, v[e], j);
+          const bool up = (g & k) == 0, lower = (g & j) == 0;
+          v[e] = (lower == up) ? min(v[e], o) : max(v[e], o);
+        } else {  // partner e ^ (j / 32) in the same lane
+          const int f = e ^ (j / 32);
+          if (f > e) {
+            const bool up = ((e * 32) & k) == 0;
+            const int a = v[e], b = v[f];
+            v[e] = up ? min(a, b) : max(a, b);
+            v[f] = up ? max(a, b) : min(a, b);
+          }
+        }
+      }
+    }
+  }
+}
+
+// Rows of the list at x, one warp per atom i: the partners j != i with
+// |x_i - x_j| <= sl (minimum image), found by walking the 27 cells around
+// i's (the lanes test a cell's atoms 32 at a time and gather the kept ones
+// in a shared buffer), then sorted ascending (warp_sort_asc, rows of up to
+// 32 E entries); x is copied to qb.  Runs only when *want != 0; clears
+// *next, the rebuild flag of the next evaluation.  A row longer than maxnb
+// (<= 32 E) sets *overflow.
+template <int E>
+__global__ void __launch_bounds__(kAB) a_rows(const double4 *x, int n, Grid g, double sl2, int maxnb, int *nbr,
+                                              int *cnt, double4 *qb, const int *want, int *next, int *overflow) {
+  __shared__ int buf[kAB / 32][32 * E];
+  const int i = (int)(((long long)blockIdx.x * kAB + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *next = 0;
+  if (i >= n || !*want) return;  // whole warps leave together
+  const double4 qi = x[i];
+  if (lane == 0) qb[i] = qi;
+  const int cx = cell_axis(qi.x, g.L[0], g.inv_cs[0], g.ms[0]);
+  const int cy = cell_axis(qi.y, g.L[1], g.inv_cs[1], g.ms[1]);
+  const int cz = cell_axis(qi.z, g.L[2], g.inv_cs[2], g.ms[2]);
+  // lane l < 27 holds cell l's first slot and the inclusive prefix of the
+  // 27 cells' counts: the candidates are one concatenated range of `total`
+  // (the row is sorted afterwards, so the walk order does not matter)
+  int beg = 0, pre = 0;
+  if (lane < 27) {
+    const int z = (cz + lane / 9 - 1 + g.ms[2]) % g.ms[2];
+    const int y = (cy + (lane / 3) % 3 - 1 + g.ms[1]) % g.ms[1];
+    const int xx = (cx + lane % 3 - 1 + g.ms[0]) % g.ms[0];
+    const int c = (z * g.ms[1] + y) * g.ms[0] + xx;
+    beg = g.start[c];
+    pre = g.start[c + 1] - beg;
+  }
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, pre, o);
+    if (lane >= o) pre += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, pre, 26);
+  int m = 0;  // partners found (warp-uniform)
+  for (int fb = 0; fb < total; fb += 32) {
+    const int f = fb + lane;
+    // the cell of candidate f: the first cell whose inclusive prefix exceeds f
+    int lo = 0, hi = 26;
+#pragma unroll
+    for (int it = 0; it < 5; it++) {
+      const int mid = (lo + hi) >> 1;
+      const int pm = __shfl_sync(0xffffffffu, pre, mid);
+      if (pm > f) hi = mid;
+      else lo = min(mid + 1, hi);
+    }
+    const int bq = __shfl_sync(0xffffffffu, beg, lo);
+    const int pp = __shfl_sync(0xffffffffu, pre, lo > 0 ? lo - 1 : 0);
+    const int excl = lo > 0 ? pp : 0;  // candidates in the cells before
+    int j = -1;
+    bool keep = false;
+    if (f < total) {
+      const int k = bq + (f - excl);
+      j = g.perm[k];
+      const double4 qj = g.qs[k];
+      double d[3] = {qi.x - qj.x, qi.y - qj.y, qi.z - qj.z};
+      for (int a = 0; a < 3; a++) d[a] -= g.L[a] * rint(d[a] * g.inv_L[a]);
+      keep = j != i && d[0] * d[0] + d[1] * d[1] + d[2] * d[2] <= sl2;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    const int slot = m + __popc(bal & ((1u << lane) - 1u));
+    if (keep && slot < maxnb) buf[wib][slot] = j;
+    m += __popc(bal);
+  }
+  __syncwarp();
+  const int mm = min(m, maxnb);
+  int v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int s = e * 32 + lane;
+    v[e] = s < mm ? buf[wib][s] : 0x7fffffff;
+  }
+  warp_sort_asc<E>(v, lane);
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int s = e * 32 + lane;
+    if (s < mm) nbr[(size_t)s * n + i] = v[e];
+  }
+  if (lane == 0) {
+    cnt[i] = mm;
+    if (m > maxnb) atomicOr(overflow, 1);
+  }
 }
 
 // --------------------------------------------------------------- physics
 template <int TPA>
-__global__ void __launch_bounds__(kAB) a_force(const double4 *q, int n, Grid g, Pot p, double4 *f) {
+__global__ void __launch_bounds__(kAB) a_force(const double4 *q, int n, Rows g, Pot p, double4 *f) {
   const int t = blockIdx.x * kAB + threadIdx.x;
   const int i = t / TPA, sub = t % TPA;
   double fx = 0.0, fy = 0.0, fz = 0.0;
   if (i < n) {
-    for_pairs<TPA>(q, g, p, i, sub, [&](int, const double *d, double r) {
+    for_pairs<TPA>(q, g, p, i, sub, n, [&](int, const double *d, double r) {
       double u, u1, u2;
       pair_u(r, p, u, u1, u2);
       const double c = -u1 / r;
@@ -251,14 +497,14 @@ __global__ void __launch_bounds__(kAB) a_force(const double4 *q, int n, Grid g, 
 // Loss terms at q: per-block sums of PE, S and dPE/dsigma (pairs counted from
 // both ends, halved); with grad, dL_t/dq_i * scale added into lq.
 template <int TPA>
-__global__ void __launch_bounds__(kAB) a_loss(const double4 *q, int n, Grid g, Pot p, double *part, double4 *lq,
+__global__ void __launch_bounds__(kAB) a_loss(const double4 *q, int n, Rows g, Pot p, double *part, double4 *lq,
                                               double scale) {
   const int t = blockIdx.x * kAB + threadIdx.x;
   const int i = t / TPA, sub = t % TPA;
   double v[3] = {0.0, 0.0, 0.0};
   double gx = 0.0, gy = 0.0, gz = 0.0;
   if (i < n) {
-    for_pairs<TPA>(q, g, p, i, sub, [&](int, const double *d, double r) {
+    for_pairs<TPA>(q, g, p, i, sub, n, [&](int, const double *d, double r) {
       double u, u1, u2, s, s1;
       pair_u(r, p, u, u1, u2);
       shell(r, p, s, s1);
@@ -289,7 +535,7 @@ __global__ void __launch_bounds__(kAB) a_loss(const double4 *q, int n, Grid g, P
 // w = H(q) u (pair energy Hessian times u); per-block sums of
 // sum_i u_i . dF_i/d(eps, sigma).
 template <int TPA>
-__global__ void __launch_bounds__(kAB) a_hvp(const double4 *q, int n, Grid g, Pot p, const double4 *u, double4 *w,
+__global__ void __launch_bounds__(kAB) a_hvp(const double4 *q, int n, Rows g, Pot p, const double4 *u, double4 *w,
                                              double *part) {
   const int t = blockIdx.x * kAB + threadIdx.x;
   const int i = t / TPA, sub = t % TPA;
@@ -297,7 +543,7 @@ __global__ void __launch_bounds__(kAB) a_hvp(const double4 *q, int n, Grid g, Po
   double wx = 0.0, wy = 0.0, wz = 0.0;
   if (i < n) {
     const double4 ui = u[i];
-    for_pairs<TPA>(q, g, p, i, sub, [&](int j, const double *d, double r) {
+    for_pairs<TPA>(q, g, p, i, sub, n, [&](int j, const double *d, double r) {
       double uu, u1, u2;
       pair_u(r, p, uu, u1, u2);
       const double4 uj = u[j];
@@ -414,6 +660,14 @@ struct Run {
   double *part = nullptr;                       // block partials of the pair kernels
   double *loss_sums = nullptr;                  // per step: PE, S, dPE/dsigma
   double *adj_sums = nullptr;                   // per reverse step: u . dF/d(eps, sigma)
+  // Verlet list (a_rows): rows, row lengths, build positions, flags (the
+  // rebuild flags of even and odd evaluations, row overflow) and a host copy
+  Rows rows{};
+  int *nbr = nullptr, *cnt = nullptr, *flag = nullptr, *hflag = nullptr;
+  double4 *qb = nullptr;
+  int maxnb = 0;
+  double sl2 = 0.0, half_skin2 = 0.0;
+  long long evals = 0;  // list preparations so far (picks the flag pair's slot)
   std::vector<void *> owned;
 
   template <typename T>
@@ -424,51 +678,81 @@ struct Run {
   }
   ~Run() {
     for (void *x : owned) cudaFree(x);
+    if (hflag) cudaFreeHost(hflag);
     if (s) cudaStreamDestroy(s);
   }
   int pair_blocks() const { return (int)(((long long)n * tpa + kAB - 1) / kAB); }
 
-  // cell grid of the positions x
-  void cells(const double4 *x) {
-    cudaMemsetAsync(count, 0, sizeof(int) * ncell, s);
-    cudaMemsetAsync(fill, 0, sizeof(int) * ncell, s);
-    a_count<<<nblk(n), kAB, 0, s>>>(x, n, g, cell, count);
-    a_scan<<<1, 1024, 0, s>>>(count, start, ncell);
-    a_fill<<<nblk(n), kAB, 0, s>>>(n, cell, start, fill, perm_fill);
-    a_sort<<<nblk(ncell * 32), kAB, 0, s>>>(ncell, start, perm_fill, perm);
-    a_gather<<<nblk(n), kAB, 0, s>>>(x, perm, qs, n);
+  // cell grid of the positions x, when *want != 0
+  void cells(const double4 *x, const int *want) {
+    if (n <= kGrid1Atoms) {
+      a_grid1<<<1, 1024, 0, s>>>(x, n, g, ncell, cell, count, start, fill, perm_fill, perm, qs, want);
+      return;
+    }
+    a_clear<<<std::min(nblk(ncell), 1024), kAB, 0, s>>>(count, fill, ncell, want);
+    a_count<<<nblk(n), kAB, 0, s>>>(x, n, g, cell, count, want);
+    a_scan<<<1, 1024, 0, s>>>(count, start, ncell, want);
+    a_fill<<<nblk(n), kAB, 0, s>>>(n, cell, start, fill, perm_fill, want);
+    a_sort<<<nblk(ncell * 32), kAB, 0, s>>>(ncell, start, perm_fill, perm, want);
+    a_gather<<<nblk(n), kAB, 0, s>>>(x, perm, qs, n, want);
+  }
+  // True if a row outgrew maxnb in any build so far (the sums are then
+  // incomplete).
+  bool rows_overflowed() {
+    if (cudaMemcpyAsync(hflag, flag + 2, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return true;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return true;
+    return hflag[0] != 0;
+  }
+  // Makes the list valid for an evaluation at x, on the device: a_check
+  // raises this evaluation's rebuild flag when an atom has moved more than
+  // skin/2 since the list's build, and the grid and row kernels run only
+  // then (two flags, used by alternate evaluations: a_rows clears the next
+  // one).  No host wait.
+  void prepare(const double4 *x) {
+    int *want = flag + (evals & 1), *next = flag + ((evals + 1) & 1);
+    evals++;
+    a_check<<<nblk(n), kAB, 0, s>>>(x, qb, n, rows, half_skin2, want);
+    cells(x, want);
+    const int wb = (int)(((long long)n * 32 + kAB - 1) / kAB);  // one warp per atom
+    int *ov = flag + 2;
+    if (maxnb <= 32) a_rows<1><<<wb, kAB, 0, s>>>(x, n, g, sl2, maxnb, nbr, cnt, qb, want, next, ov);
+    else if (maxnb <= 64) a_rows<2><<<wb, kAB, 0, s>>>(x, n, g, sl2, maxnb, nbr, cnt, qb, want, next, ov);
+    else if (maxnb <= 128) a_rows<4><<<wb, kAB, 0, s>>>(x, n, g, sl2, maxnb, nbr, cnt, qb, want, next, ov);
+    else if (maxnb <= 256) a_rows<8><<<wb, kAB, 0, s>>>(x, n, g, sl2, maxnb, nbr, cnt, qb, want, next, ov);
+    else if (maxnb <= 512) a_rows<16><<<wb, kAB, 0, s>>>(x, n, g, sl2, maxnb, nbr, cnt, qb, want, next, ov);
+    else a_rows<32><<<wb, kAB, 0, s>>>(x, n, g, sl2, maxnb, nbr, cnt, qb, want, next, ov);
   }
   void force(const double4 *x) {
     const int nb = pair_blocks();
     switch (tpa) {
-      case 1: a_force<1><<<nb, kAB, 0, s>>>(x, n, g, p, f); break;
-      case 2: a_force<2><<<nb, kAB, 0, s>>>(x, n, g, p, f); break;
-      case 4: a_force<4><<<nb, kAB, 0, s>>>(x, n, g, p, f); break;
-      default: a_force<8><<<nb, kAB, 0, s>>>(x, n, g, p, f); break;
+      case 1: a_force<1><<<nb, kAB, 0, s>>>(x, n, rows, p, f); break;
+      case 2: a_force<2><<<nb, kAB, 0, s>>>(x, n, rows, p, f); break;
+      case 4: a_force<4><<<nb, kAB, 0, s>>>(x, n, rows, p, f); break;
+      default: a_force<8><<<nb, kAB, 0, s>>>(x, n, rows, p, f); break;
     }
   }
   void loss(const double4 *x, double4 *grad, double scale) {
     const int nb = pair_blocks();
     switch (tpa) {
-      case 1: a_loss<1><<<nb, kAB, 0, s>>>(x, n, g, p, part, grad, scale); break;
-      case 2: a_loss<2><<<nb, kAB, 0, s>>>(x, n, g, p, part, grad, scale); break;
-      case 4: a_loss<4><<<nb, kAB, 0, s>>>(x, n, g, p, part, grad, scale); break;
-      default: a_loss<8><<<nb, kAB, 0, s>>>(x, n, g, p, part, grad, scale); break;
+      case 1: a_loss<1><<<nb, kAB, 0, s>>>(x, n, rows, p, part, grad, scale); break;
+      case 2: a_loss<2><<<nb, kAB, 0, s>>>(x, n, rows, p, part, grad, scale); break;
+      case 4: a_loss<4><<<nb, kAB, 0, s>>>(x, n, rows, p, part, grad, scale); break;
+      default: a_loss<8><<<nb, kAB, 0, s>>>(x, n, rows, p, part, grad, scale); break;
     }
   }
   void hvp(const double4 *x) {
     const int nb = pair_blocks();
     switch (tpa) {
-      case 1: a_hvp<1><<<nb, kAB, 0, s>>>(x, n, g, p, u, w, part); break;
-      case 2: a_hvp<2><<<nb, kAB, 0, s>>>(x, n, g, p, u, w, part); break;
-      case 4: a_hvp<4><<<nb, kAB, 0, s>>>(x, n, g, p, u, w, part); break;
-      default: a_hvp<8><<<nb, kAB, 0, s>>>(x, n, g, p, u, w, part); break;
+      case 1: a_hvp<1><<<nb, kAB, 0, s>>>(x, n, rows, p, u, w, part); break;
+      case 2: a_hvp<2><<<nb, kAB, 0, s>>>(x, n, rows, p, u, w, part); break;
+      case 4: a_hvp<4><<<nb, kAB, 0, s>>>(x, n, rows, p, u, w, part); break;
+      default: a_hvp<8><<<nb, kAB, 0, s>>>(x, n, rows, p, u, w, part); break;
     }
   }
   // one forward step; keeps q_h and v' when asked
   void step(double4 *qh_out, double4 *v_out) {
     a_drift<<<nblk(n), kAB, 0, s>>>(q, v, n, 0.5 * dt);
-    cells(q);
+    prepare(q);
     force(q);
     if (qh_out) cudaMemcpyAsync(qh_out, q, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
     a_kick<<<nblk(n), kAB, 0, s>>>(v, f, n, dt);
@@ -477,7 +761,7 @@ struct Run {
   }
   // loss terms at x: sums into out[0..2] (device), gradient into lq when scale != 0
   void loss_at(const double4 *x, double scale, double *out) {
-    cells(x);
+    prepare(x);
     loss(x, scale != 0.0 ? lq : nullptr, scale);
     if (out) a_reduce<<<1, kRB, 0, s>>>(part, pair_blocks(), 3, out);
   }
@@ -500,7 +784,7 @@ int autotune_tpa(Run &R, int device) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  R.cells(R.q);
+  R.prepare(R.q);
   int best = 1;
   float best_ms = 1e30f;
   for (int t : {1, 2, 4, 8}) {
@@ -563,14 +847,41 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   R.n = n;
   R.dt = prm->time_step;
   const double rc = prm->cutoff * prm->sigma;
+  // list skin: 0.3 sigma, less where a box axis holds fewer than three
+  // cells of r_c + skin (no skin at all: the list is rebuilt whenever an
+  // atom moved)
+  double skin = 0.3 * prm->sigma;
   for (int d = 0; d < 3; d++) {
     const double L = prm->L[d];
     if (!(L > 0.0) || !std::isfinite(L)) return MDG_ERR_INVALID_ARGUMENT;
-    R.g.ms[d] = (int)(L / rc);
-    if (R.g.ms[d] < 3) return MDG_ERR_BOX_TOO_SMALL;
+    if ((int)(L / rc) < 3) return MDG_ERR_BOX_TOO_SMALL;
+    skin = std::min(skin, L / 3.0 * (1.0 - 1e-9) - rc);  // cells of L/ms >= r_c + skin, ms >= 3
+  }
+  skin = std::max(skin, 0.0);
+  const double sl = rc + skin;
+  for (int d = 0; d < 3; d++) {
+    const double L = prm->L[d];
+    R.g.ms[d] = std::max(3, (int)(L / sl));
     R.g.L[d] = L;
     R.g.inv_cs[d] = R.g.ms[d] / L;
     R.g.inv_L[d] = 1.0 / L;
+    R.rows.L[d] = L;
+    R.rows.inv_L[d] = 1.0 / L;
+  }
+  // rows keep pairs up to sl, a hair wider than the r_c + 2 (skin / 2) that
+  // the displacement bound needs
+  R.sl2 = sl * sl * (1.0 + 1e-9);
+  R.half_skin2 = 0.25 * skin * skin;
+  {
+    const double vol = prm->L[0] * prm->L[1] * prm->L[2];
+    const double est = 4.0 / 3.0 * M_PI * sl * sl * sl * (double)n / vol;
+    // twice the mean density's count plus 64, and at least the count at
+    // density 1.3 (above a close-packed LJ solid) plus 32, so that a dense
+    // region of a dilute box fits; at most 1024 (the row sort's width).  A
+    // longer row is MDG_ERR_CAPACITY.
+    const double dense = 4.0 / 3.0 * M_PI * sl * sl * sl * 1.3 / (prm->sigma * prm->sigma * prm->sigma);
+    const double want = std::max(std::ceil(2.0 * est + 64.0), std::ceil(dense + 32.0));
+    R.maxnb = (int)std::min<double>(std::min(std::max(n - 1, 1), 1024), want);
   }
   R.ncell = R.g.ms[0] * R.g.ms[1] * R.g.ms[2];
   const double sc = prm->cutoff;
@@ -605,6 +916,17 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   if (e == cudaSuccess) e = R.alloc(&R.qs, n);
   if (e == cudaSuccess) e = R.alloc(&R.part, max_blocks * 3);
   if (e == cudaSuccess) e = R.alloc(&R.loss_sums, (size_t)T * 3);
+  if (e == cudaSuccess) e = R.alloc(&R.nbr, (size_t)R.maxnb * n);
+  if (e == cudaSuccess) e = R.alloc(&R.cnt, n);
+  if (e == cudaSuccess) e = R.alloc(&R.qb, n);
+  if (e == cudaSuccess) e = R.alloc(&R.flag, 3);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&R.hflag, 2 * sizeof(int));
+  if (e == cudaSuccess) {
+    const int first[3] = {1, 0, 0};  // the first evaluation builds the list; no overflow
+    e = cudaMemsetAsync(R.qb, 0, sizeof(double4) * n, R.s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(R.flag, first, sizeof(first), cudaMemcpyHostToDevice, R.s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(R.s);
+  }
   if (grad) {
     if (e == cudaSuccess) e = R.alloc(&R.lq, n);
     if (e == cudaSuccess) e = R.alloc(&R.lv, n);
@@ -620,6 +942,8 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   R.g.start = R.start;
   R.g.perm = R.perm;
   R.g.qs = R.qs;
+  R.rows.nbr = R.nbr;
+  R.rows.cnt = R.cnt;
 
   // upload (n x 3 host arrays -> double4)
   {
@@ -656,7 +980,7 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
     dl_dsig += sums[3 * t + 2];
   }
   *loss = l * norm;
-  if (!grad) return MDG_OK;
+  if (!grad) return R.rows_overflowed() ? MDG_ERR_CAPACITY : MDG_OK;
   dl_deps *= norm;
   dl_dsig *= norm;
 
@@ -676,7 +1000,7 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
       a_drift<<<nblk(n), kAB, 0, R.s>>>(R.tmp, vp, n, 0.5 * R.dt);
       R.loss_at(R.tmp, norm, nullptr);
       a_rev1<<<nblk(n), kAB, 0, R.s>>>(R.lq, R.lv, R.u, n, R.dt);
-      R.cells(qh);
+      R.prepare(qh);
       R.hvp(qh);
       a_reduce<<<1, kRB, 0, R.s>>>(R.part, R.pair_blocks(), 2, R.adj_sums + (size_t)2 * t);
       a_rev2<<<nblk(n), kAB, 0, R.s>>>(R.lq, R.lv, R.w, n, R.dt);
@@ -702,7 +1026,7 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   }
   if (dloss_deps) *dloss_deps = dl_deps;
   if (dloss_dsigma) *dloss_dsigma = dl_dsig;
-  return MDG_OK;
+  return R.rows_overflowed() ? MDG_ERR_CAPACITY : MDG_OK;
 }
 
 }  // extern "C"

@@ -148,8 +148,8 @@ def test_rejects_box_below_three_cells():
 
 @pytest.mark.gpu
 def test_lanes_per_atom_only_regroup_the_sums():
-    # 1, 2, 4 or 8 lanes per atom split each atom's 27 cells differently, so
-    # only the grouping of the FP64 sums changes
+    # 1, 2, 4 or 8 lanes per atom split each atom's row differently (lane =
+    # partner index mod lanes), so only the grouping of the FP64 sums changes
     q0, v0, L = small_state()
     runs = [_gpu_grads(q0, v0, L, steps=40, checkpoint_every=10, threads_per_atom=t) for t in (1, 2, 4, 8)]
     for r in runs[1:]:
