@@ -457,12 +457,18 @@ typedef struct mdg_adjoint_params {
 void mdg_adjoint_default_params(mdg_adjoint_params *p);
 /* q0, v0: n x 3 doubles.  loss is required; with all three gradient
  * pointers NULL only the forward pass runs.  dloss_dq0: n x 3 doubles.
- * Allocates its device memory per call (checkpoints: 2 x 32 B per atom per
- * checkpoint; the list: 4 B per row entry, rows of up to 1024 entries).
+ * Device memory (checkpoints: 2 x 32 B per atom per checkpoint; the list:
+ * 4 B per row entry, rows of up to 1024 entries) is kept per device after
+ * the call and reused by later calls whose buffers fit, so repeated calls of
+ * one shape allocate nothing; one run at a time per process.
  * MDG_ERR_CAPACITY if a row outgrows its capacity (three times the mean
  * density's count within the search length, plus 64). */
 mdg_status mdg_adjoint_run(const mdg_adjoint_params *p, const double *q0, const double *v0, int n, double *loss,
                            double *dloss_deps, double *dloss_dsigma, double *dloss_dq0);
+/* Frees the device memory, stream and pinned buffer that mdg_adjoint_run
+ * keeps between calls (all devices).  Call it before cudaDeviceReset; a run
+ * after a reset without it finds its kept buffers gone and allocates anew. */
+void mdg_adjoint_release(void);
 
 const char *mdg_last_error(mdg_handle *h);
 const char *mdg_status_string(mdg_status s);

@@ -169,6 +169,7 @@ _I64P = ctypes.POINTER(ctypes.c_int64)
 SIGNATURES = {
     "mdg_adjoint_default_params": (None, [ctypes.POINTER(AdjointParams)]),
     "mdg_adjoint_run": (ctypes.c_int, [ctypes.POINTER(AdjointParams), _DP, _DP, ctypes.c_int, _DP, _DP, _DP, _DP]),
+    "mdg_adjoint_release": (None, []),
     "mdg_default_params": (None, [ctypes.POINTER(Params)]),
     "mdg_set_external": (ctypes.c_int, [_H, ctypes.POINTER(External)]),
     "mdg_change_scale": (ctypes.c_int, [_H, ctypes.c_double]),

@@ -79,6 +79,11 @@ def trajectory_gradients(q0, v0, L, **kw):
     return _run(params(L, **kw), q0, v0, grad=True)
 
 
+def release():
+    """Frees the device memory the adjoint keeps between runs (mdg_adjoint_release)."""
+    load_library().mdg_adjoint_release()
+
+
 try:
     import torch
 

@@ -645,7 +645,31 @@ __global__ void a_rev2(double4 *lq, double4 *lv, const double4 *w, int n, double
 
 int nblk(int n) { return n > 0 ? (n + kAB - 1) / kAB : 1; }
 
+// Device buffers, stream and pinned flag copy of the adjoint, kept per
+// device between calls: a call takes its buffers in a fixed order and reuses
+// every kept buffer that is large enough, replacing the others, so repeated
+// calls of one shape allocate nothing.  One run at a time per process
+// (g_ws_mutex); mdg_adjoint_release frees everything.
+struct Workspace {
+  std::vector<void *> buf;
+  std::vector<size_t> bytes;
+  cudaStream_t s = nullptr;
+  int *hflag = nullptr;
+};
+std::mutex g_ws_mutex;
+std::map<int, Workspace> g_ws;
+
+void free_workspace(Workspace &w) {
+  for (void *x : w.buf)
+    if (x) cudaFree(x);
+  if (w.hflag) cudaFreeHost(w.hflag);
+  if (w.s) cudaStreamDestroy(w.s);
+  w = Workspace();
+}
+
 struct Run {
+  Workspace *ws = nullptr;
+  size_t slot = 0;  // next workspace buffer
   int n = 0, ncell = 0, tpa = 1;
   cudaStream_t s = nullptr;
   Grid g{};
@@ -668,18 +692,26 @@ struct Run {
   int maxnb = 0;
   double sl2 = 0.0, half_skin2 = 0.0;
   long long evals = 0;  // list preparations so far (picks the flag pair's slot)
-  std::vector<void *> owned;
 
   template <typename T>
   cudaError_t alloc(T **ptr, size_t count_) {
-    cudaError_t e = cudaMalloc((void **)ptr, sizeof(T) * (count_ ? count_ : 1));
-    if (e == cudaSuccess) owned.push_back(*ptr);
-    return e;
-  }
-  ~Run() {
-    for (void *x : owned) cudaFree(x);
-    if (hflag) cudaFreeHost(hflag);
-    if (s) cudaStreamDestroy(s);
+    const size_t b = sizeof(T) * (count_ ? count_ : 1);
+    if (slot == ws->buf.size()) {
+      ws->buf.push_back(nullptr);
+      ws->bytes.push_back(0);
+    }
+    if (ws->bytes[slot] < b) {
+      if (ws->buf[slot]) cudaFree(ws->buf[slot]);
+      ws->buf[slot] = nullptr;
+      ws->bytes[slot] = 0;
+      void *p = nullptr;
+      const cudaError_t e = cudaMalloc(&p, b);
+      if (e != cudaSuccess) return e;
+      ws->buf[slot] = p;
+      ws->bytes[slot] = b;
+    }
+    *ptr = static_cast<T *>(ws->buf[slot++]);
+    return cudaSuccess;
   }
   int pair_blocks() const { return (int)(((long long)n * tpa + kAB - 1) / kAB); }
 
@@ -812,6 +844,17 @@ int autotune_tpa(Run &R, int device) {
 
 extern "C" {
 
+void mdg_adjoint_release(void) {
+  std::lock_guard<std::mutex> lock(g_ws_mutex);
+  int cur = 0;
+  const bool have = cudaGetDevice(&cur) == cudaSuccess;
+  for (auto &kv : g_ws) {
+    if (cudaSetDevice(kv.first) == cudaSuccess) free_workspace(kv.second);
+  }
+  g_ws.clear();
+  if (have) cudaSetDevice(cur);
+}
+
 void mdg_adjoint_default_params(mdg_adjoint_params *p) {
   if (!p) return;
   memset(p, 0, sizeof(*p));
@@ -902,7 +945,23 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   const int nck = (T + k - 1) / k + 1;
   const size_t max_blocks = ((size_t)n * 8 + kAB - 1) / kAB;
 
-  cudaError_t e = cudaStreamCreateWithFlags(&R.s, cudaStreamNonBlocking);
+  std::lock_guard<std::mutex> ws_lock(g_ws_mutex);
+  Workspace &ws = g_ws[prm->device];
+  if (!ws.buf.empty()) {
+    // buffers of an earlier call: still this context's device memory? (a
+    // device reset in between drops them)
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, ws.buf[0]) != cudaSuccess || at.type != cudaMemoryTypeDevice) {
+      cudaGetLastError();
+      ws = Workspace();
+    }
+  }
+  R.ws = &ws;
+  cudaError_t e = cudaSuccess;
+  if (!ws.s) e = cudaStreamCreateWithFlags(&ws.s, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !ws.hflag) e = cudaMallocHost((void **)&ws.hflag, 2 * sizeof(int));
+  R.s = ws.s;
+  R.hflag = ws.hflag;
   if (e == cudaSuccess) e = R.alloc(&R.q, n);
   if (e == cudaSuccess) e = R.alloc(&R.v, n);
   if (e == cudaSuccess) e = R.alloc(&R.f, n);
@@ -920,7 +979,6 @@ mdg_status mdg_adjoint_run(const mdg_adjoint_params *prm, const double *q0, cons
   if (e == cudaSuccess) e = R.alloc(&R.cnt, n);
   if (e == cudaSuccess) e = R.alloc(&R.qb, n);
   if (e == cudaSuccess) e = R.alloc(&R.flag, 3);
-  if (e == cudaSuccess) e = cudaMallocHost((void **)&R.hflag, 2 * sizeof(int));
   if (e == cudaSuccess) {
     const int first[3] = {1, 0, 0};  // the first evaluation builds the list; no overflow
     e = cudaMemsetAsync(R.qb, 0, sizeof(double4) * n, R.s);

@@ -139,6 +139,27 @@ def test_autograd_function_backpropagates():
 
 
 @pytest.mark.gpu
+def test_repeated_runs_reuse_the_kept_device_memory():
+    # the second run of a shape allocates nothing (device free memory is
+    # unchanged) and gives the same numbers; release() frees the workspace
+    # and the next run allocates it again
+    from mdacp_b200 import adjoint as A
+    q0, v0, L = small_state(ncell=8)  # 2,048 atoms
+    kw = dict(steps=60, checkpoint_every=10)
+    a = _gpu_grads(q0, v0, L, **kw)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    b = _gpu_grads(q0, v0, L, **kw)
+    torch.cuda.synchronize()
+    free2, _ = torch.cuda.mem_get_info()
+    assert free2 == free1
+    assert a[0] == b[0] and a[1] == b[1] and a[2] == b[2] and np.array_equal(a[3], b[3])
+    A.release()
+    c = _gpu_grads(q0, v0, L, **kw)
+    assert c[0] == a[0] and np.array_equal(c[3], a[3])
+
+
+@pytest.mark.gpu
 def test_rejects_box_below_three_cells():
     from mdacp_b200 import MdgError
     q0, v0, L = small_state(ncell=3)  # L = 5.04 < 3 cut-offs
