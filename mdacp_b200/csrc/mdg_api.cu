@@ -1077,11 +1077,11 @@ mdg_status mdg_set_state(mdg_handle *h, const double *q4, const double *v4, cons
   if (n > 0) {
     CUDA_TRY(h, cudaMemcpyAsync(h->a.q, q4, sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, cudaMemcpyAsync(h->a.v, v4, sizeof(double4) * n, cudaMemcpyHostToDevice, h->stream));
-    std::vector<int> ids(n), ty(n, 0);
-    for (int i = 0; i < n; i++) ids[i] = i;
-    if (type) std::copy(type, type + n, ty.begin());
-    CUDA_TRY(h, cudaMemcpyAsync(h->a.ids, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
-    CUDA_TRY(h, cudaMemcpyAsync(h->a.type, ty.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    // upload indices made on the device; types copied from the caller's
+    // array (0 without one)
+    k_upload_ids<kBlock><<<blocks_for(n, kBlock), kBlock, 0, h->stream>>>(h->a, n);
+    if (type) CUDA_TRY(h, cudaMemcpyAsync(h->a.type, type, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    else CUDA_TRY(h, cudaMemsetAsync(h->a.type, 0, sizeof(int) * n, h->stream));
     if (h->prm.max_neighbors <= 0 && (!h->a.nbr || n != h->n)) {
       mdg_status r = alloc_neighbors(h, estimate_max_neighbors(h, q4, n));
       if (r) return r;

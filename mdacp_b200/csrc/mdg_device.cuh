@@ -262,6 +262,13 @@ __device__ __forceinline__ double image_of(double xj, double xi, double L, doubl
 }
 
 // ---------------------------------------------------------------- kernels
+// Upload indices of a fresh state: slot i holds atom i.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_upload_ids(Arrays a, int n) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  if (i < n) a.ids[i] = i;
+}
+
 // Initial |v|^2 maximum (used before the first step after an upload) and a
 // finiteness check of the uploaded state.
 template <int BLOCK>
