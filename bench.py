@@ -180,8 +180,9 @@ def run_reference_bench(state, steps, warmup, threads, config):
 
 
 def ref_sample_steps(cores, seconds, n):
-    # about 2.6e6 atom-steps/s per core for the AVX2 build at rho 0.84, rc 2.5
-    est = 2.6e6 * cores
+    # about 5e6 atom-steps/s per core for the AVX2 build at rho 0.84, rc 2.5
+    # (8.1e7-8.6e7 measured on 16 host cores of the B200 box)
+    est = 5.0e6 * cores
     return int(min(2000, max(10, seconds * est / n)))
 
 
