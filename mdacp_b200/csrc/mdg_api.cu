@@ -150,7 +150,7 @@ cudaError_t dalloc(T **p, size_t count) {
 void free_arrays(Arrays &a) {
   void *ptrs[] = {a.q, a.v, a.q_old, a.qfix, a.qfix2, a.qloc, a.cxyz, a.xsub, a.ids, a.type, a.cell, a.nbr, a.nnbr, a.cell_count,
                   a.cell_start, a.slot, a.perm, a.perm2, a.q_tmp, a.v_tmp, a.v_lag, a.ids_tmp, a.type_tmp,
-                  a.cell_tmp, a.mult, a.cand, a.partials, a.st, a.stage_rng, a.stage_n, a.nbr16};
+                  a.cell_tmp, a.mult, a.cand, a.partials, a.st, a.stage_rng, a.stage_n, a.nbr16, a.disp2};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   a = Arrays{};
@@ -1005,6 +1005,7 @@ mdg_status mdg_create(const mdg_params *prm, mdg_handle **out) {
   if (e == cudaSuccess) e = dalloc(&a.perm, cap);
   if (e == cudaSuccess) e = dalloc(&a.perm2, cap);
   if (e == cudaSuccess) e = dalloc(&a.q_tmp, cap);
+  if (e == cudaSuccess) e = dalloc(&a.disp2, cap);
   if (e == cudaSuccess) e = dalloc(&a.v_tmp, cap);
   if (e == cudaSuccess) e = dalloc(&a.v_lag, cap);
   if (e == cudaSuccess) e = dalloc(&a.ids_tmp, cap);

@@ -140,6 +140,7 @@ struct Arrays {
   int *ids_tmp, *type_tmp, *cell_tmp;
   unsigned char *mult; // ghost-border membership at the last build (bits, see border_bits)
   int2 *cand;         // displacement-check candidates: (slot, image code)
+  double *disp2;      // per atom: the largest squared copy displacement of the last skin check (k_disp_max); null: not kept
   double *partials;   // per-block partial sums for reductions
   Status *st;
   int stride;         // column stride of nbr (>= cap, multiple of 32)
@@ -444,6 +445,7 @@ __global__ void __launch_bounds__(BLOCK) k_disp_max(Arrays a, Box b, int n, doub
   const int i = blockIdx.x * BLOCK + threadIdx.x;
   double d2 = 0.0;
   if (i < n) for_each_copy(copy_view(a), b.L, i, lag, [&](int, double x) { d2 = fmax(d2, x); });
+  if (a.disp2 && i < n) a.disp2[i] = d2;
   block_max_to<BLOCK>(&a.st->dr2max_bits, d2);
 }
 
@@ -455,6 +457,9 @@ __global__ void __launch_bounds__(BLOCK) k_disp_collect(Arrays a, Box b, int n, 
   if (i >= n) return;
   const double c = b.buffer_length - sqrt(__longlong_as_double((long long)a.st->dr2max_bits));
   const double c_d2 = c * c;
+  // no copy of this atom moved more than c (k_disp_max's per-atom maximum
+  // of the same displacements): nothing to collect
+  if (a.disp2 && !(a.disp2[i] > c_d2)) return;
   for_each_copy(copy_view(a), b.L, i, lag, [&](int code, double d2) {
     if (d2 > c_d2) {
       atomicAdd(&a.st->cand_weighted, 1);
