@@ -82,6 +82,7 @@ struct Ens {
   int *ids_tmp;
   unsigned char *mult;
   int2 *cand;  // nrep x cll candidate copies (slot, image code)
+  double *disp2;  // per atom: the largest squared copy displacement of the last skin check (ke_disp_max)
   int *error;
   double *sums;  // nrep x 3 observer sums
   WorkList wd, wb;  // skin-check and rebuild work lists
@@ -279,6 +280,7 @@ __global__ void __launch_bounds__(kEB) ke_disp_max(Ens e) {
     if (active) {
       const int i = work_atom(e, e.wd, g, &r);
       for_each_copy(ens_view(e), e.rep[r].L, i, e.lag, [&](int, double x) { d2 = fmax(d2, x); });
+      e.disp2[i] = d2;
     }
     rep_max(&e.rs[0].dr2max_bits, sizeof(RepStatus), r, d2, active);
   }
@@ -292,6 +294,9 @@ __global__ void __launch_bounds__(kEB) ke_disp_collect(Ens e) {
     RepStatus &st = e.rs[r];
     const double c = e.rep[r].buffer_length - sqrt(__longlong_as_double((long long)st.dr2max_bits));
     const double c_d2 = c * c;
+    // no copy of this atom moved more than c (ke_disp_max's per-atom
+    // maximum of the same displacements): nothing to collect
+    if (!(e.disp2[i] > c_d2)) continue;
     for_each_copy(ens_view(e), e.rep[r].L, i, e.lag, [&](int code, double d2) {
       if (d2 > c_d2) {
         atomicAdd(&st.cand_weighted, 1);
@@ -795,7 +800,7 @@ void e_free(mdg_ensemble *x) {
   Ens &e = x->e;
   void *ptrs[] = {(void *)e.rep, e.rs, (void *)e.rep_of, e.q, e.v, e.q_old, e.qfix, e.qloc, e.cxyz, e.xsub, e.ids, e.cell,
                   e.cell_tmp, e.nbr, e.nnbr, e.cell_count, e.cell_start, e.slot, e.perm, e.perm2, e.q_tmp,
-                  e.v_tmp, e.ids_tmp, e.mult, e.cand, e.error, e.sums, x->d_flags, x->d_count,
+                  e.v_tmp, e.ids_tmp, e.mult, e.cand, e.disp2, e.error, e.sums, x->d_flags, x->d_count,
                   x->d_lists};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1170,6 +1175,7 @@ mdg_status mdg_ensemble_create(const mdg_params *prm, int nrep, const mdg_replic
   if (err == cudaSuccess) err = edalloc(&e.ids_tmp, n);
   if (err == cudaSuccess) err = edalloc(&e.mult, n);
   if (err == cudaSuccess) err = edalloc(&e.cand, (size_t)nrep * e.cll);
+  if (err == cudaSuccess) err = edalloc(&e.disp2, n);
   if (err == cudaSuccess) err = edalloc(&e.error, 1);
   if (err == cudaSuccess) err = edalloc(&e.sums, (size_t)3 * nrep);
   if (err == cudaSuccess) err = edalloc(&x->d_flags, 4);
